@@ -1,0 +1,133 @@
+/*
+ * jqc.h -- C ABI of libjqc.so, the B200 (sm_100a) two-electron engine behind
+ * the jax_qc drop-in (jax_examples_b200).
+ *
+ * Conventions
+ *   - Every entry point returns an int status (JQC_OK = 0); on failure
+ *     jqc_last_error() returns a message for the calling thread.
+ *   - Basis data is passed as HOST arrays; matrices (D, J, K, S, T, V,
+ *     gradients, ERI tensors, Boys inputs/outputs) are DEVICE pointers on the
+ *     context's device, row-major float64 unless stated.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Entry points
+ *     that only launch work on `stream` are asynchronous; the ones that say
+ *     "synchronizes" wait for `stream`.
+ *   - Layout: basis functions in shell order, Cartesian components of a shell
+ *     in libint order (lx descending, then ly descending), as
+ *     jax_qc/integrals/mcmurchie_davidson.py:39-50 and overlap.py:58-64.
+ */
+#ifndef JQC_H_
+#define JQC_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JQC_OK 0
+#define JQC_ERR_INVALID 1      /* bad argument (maps to ValueError)           */
+#define JQC_ERR_CUDA 2         /* CUDA runtime failure                        */
+#define JQC_ERR_TOO_LARGE 3    /* output would exceed the size cap            */
+#define JQC_ERR_NOT_READY 4    /* call order violated (basis/pairs missing)   */
+#define JQC_ERR_UNSUPPORTED 5  /* angular momentum or class not supported     */
+#define JQC_ERR_TIMEOUT 6      /* a bounded device wait gave up               */
+
+#define JQC_PREC_FP64 0        /* every quartet in FP64 (the plain kernel)    */
+#define JQC_PREC_MIXED 1       /* Q_ij*Q_kl < mixed_tau in FP32, rest FP64    */
+#define JQC_PREC_FP32 2        /* every quartet in FP32 (test/diagnostics)    */
+
+typedef struct jqc_ctx jqc_ctx;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *jqc_last_error(void);
+
+/* ABI version (major*100 + minor). */
+int jqc_version(void);
+
+/* Create / destroy an engine context bound to CUDA device `device`.
+ * Replaces the implicit global state of jax_qc.integrals (integrals/eri.py:69). */
+int jqc_ctx_create(int device, jqc_ctx **out);
+int jqc_ctx_destroy(jqc_ctx *ctx);
+
+/* Upload a contracted Cartesian basis: shell s has angular momentum l[s]
+ * (0..2), nprim[s] primitives starting at prim_off[s] in exps/coefs
+ * (coefficients already normalized as jax_qc/basis/normalize.py:91-107 does),
+ * centre centres[3s..3s+2] (bohr), atom atom_of_shell[s].  Atoms: n_atom
+ * positions atom_xyz[3a..] and nuclear charges atom_charge[a].  cartesian must
+ * be 1 (spherical sets are transformed on the host).  Mirrors the BasisSet /
+ * Molecule inputs of compute_integrals (integrals/interface.py:26-67). */
+int jqc_basis_upload(jqc_ctx *ctx, int n_shell, const int *l, const int *nprim, const int *prim_off,
+                     const double *exps, const double *coefs, const double *centres, const int *atom_of_shell,
+                     int n_atom, const double *atom_xyz, const double *atom_charge, int cartesian);
+
+/* Build shell-pair data (Gaussian products, E-coefficient inputs) and the
+ * Schwarz bounds Q_ij = sqrt(max (ij|ij)) on the device; drop pairs that can
+ * never pass Q_ij * max Q >= schwarz_tau.  Synchronizes `stream`.
+ * Replaces integrals/screening.py:32-58 (compute_shell_pair_bounds). */
+int jqc_pairs_build(jqc_ctx *ctx, double schwarz_tau, void *stream);
+
+/* Counters of the work list for (precision_mode, mixed_tau) as jqc_jk
+ * would use it: out[0] shell pairs, out[1] kept pairs, out[2] screened
+ * canonical quartets on the FP64 path, out[3] on the FP32 path, out[4]
+ * primitive quartets (both), out[5] Cartesian basis functions, out[6] warp
+ * tasks, out[7] kernel launches per jqc_jk call.  No reference counterpart
+ * (the reference never screens: integrals/screening.py is unused). */
+int jqc_stats(jqc_ctx *ctx, int precision_mode, double mixed_tau, long long *out8);
+
+/* Per-class counters: for p in {FP64, FP32 path} and the 21 quartet classes
+ * (bra pair class >= ket pair class, pair classes ss ps pp ds dp dd),
+ * out[(p*21+q)*3 + 0..2] = canonical quartets, primitive quartets, tasks.
+ * No reference counterpart (feeds the FLOP model of the roofline). */
+int jqc_class_stats(jqc_ctx *ctx, int precision_mode, double mixed_tau, long long *out126);
+
+/* Schwarz matrix Q (n_shell x n_shell, device) in original shell order.
+ * Replaces integrals/screening.py:32-58. */
+int jqc_schwarz(jqc_ctx *ctx, double *Q, void *stream);
+
+/* Boys function F_m(T), m = 0..mmax (mmax <= 16) for n values T (device);
+ * out is n x (mmax+1), float64 or (fp32 != 0) float32.
+ * Replaces integrals/boys.py:34-109 (boys_f0 / boys_fn). */
+int jqc_boys(const double *T, long long n, int mmax, void *out, int fp32, void *stream);
+
+/* Primitive Cartesian ERI blocks for n primitive quartets of one class
+ * (la lb | lc ld) with la >= lb, lc >= ld, (la,lb) >= (lc,ld): exps is n x 4,
+ * centres n x 12 (device); out is n x nc_a nc_b nc_c nc_d.
+ * Replaces integrals/obara_saika.py:227-332 (primitive_eri_block). */
+int jqc_eri_prim_quartets(int la, int lb, int lc, int ld, long long n, const double *exps, const double *centres,
+                          double *out, void *stream);
+
+/* Dense (n,n,n,n) ERI tensor over the kept shell pairs (exact when pairs
+ * were built with schwarz_tau = 0).  Fails with JQC_ERR_TOO_LARGE when
+ * n^4 * 8 bytes exceeds `max_bytes`.
+ * Replaces integrals/eri.py:69-138 (compute_eri_tensor). */
+int jqc_eri_tensor(jqc_ctx *ctx, double *out_n4, long long max_bytes, void *stream);
+
+/* One-electron matrices S, T, V (n x n each, device) of the uploaded basis
+ * and nuclei.  Replaces integrals/overlap.py:67-85, kinetic.py:42-59 and
+ * nuclear.py:62-81 (compute_overlap/kinetic/nuclear_matrix). */
+int jqc_one_electron(jqc_ctx *ctx, double *S, double *T, double *V, void *stream);
+
+/* Direct J/K (the N^4 tensor is never stored): for each of n_dens densities
+ * D[d] (n x n, symmetric), J[d] = sum_ls D_ls (mn|ls), K[d] = sum_ls D_ls
+ * (ms|ln).  precision_mode as JQC_PREC_*, mixed_tau the FP32/FP64 split on
+ * Q_ij*Q_kl, dens_tau the density-weighted skip threshold (0 = off).
+ * Replaces scf/fock.py:31-38 (_coulomb / _exchange) and the J/K of
+ * build_fock_rhf / build_fock_uhf (fock.py:41-79) and guess.py:87-88. */
+int jqc_jk(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode, double mixed_tau,
+           double dens_tau, void *stream);
+
+/* jqc_jk with the class kernels run one after another on `stream`, each
+ * timed with CUDA events; class_ms[p*21+q] receives milliseconds (0 for
+ * empty classes).  Synchronizes.  Measurement variant of jqc_jk. */
+int jqc_jk_timed(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode,
+                 double mixed_tau, double dens_tau, void *stream, double *class_ms);
+
+/* FMA throughput microbenchmark on the current device: `blocks` blocks of
+ * 256 threads, each 8 independent FMA chains of 16*iters steps, FP64 or
+ * FP32; *tflops = achieved TFLOP/s.  Synchronizes.  No reference
+ * counterpart (roofline denominator for the compute-bound kernels). */
+int jqc_fp_peak(int fp32, int blocks, int iters, double *tflops, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JQC_H_ */

@@ -1,0 +1,97 @@
+// Boys function F_m(T) = int_0^1 u^{2m} exp(-T u^2) du on the device.
+//
+// Method (our own; the reference's boys_fn at jax_qc/integrals/boys.py:86-109
+// uses upward recurrence, which is unstable for m >= 3 at small T):
+//   T < 36:  F_M(T) from a table of F_m(T_i) on the grid T_i = i/16 by the
+//            Taylor series  F_M(T_i - d) = sum_k F_{M+k}(T_i) d^k / k!
+//            (|d| <= 1/32; 8 terms in FP64 (truncation ~2e-17 relative),
+//            5 terms in FP32), then the stable downward recursion
+//            F_{m-1} = (2T F_m + e^{-T}) / (2m-1).
+//   T >= 36: F_0 = sqrt(pi/T)/2 (erf(6) = 1 to 2e-17), then upward
+//            recursion F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T), well
+//            conditioned for T > m.
+// The table (kBoysRows x kBoysCols, row-major by T) is computed on the host
+// in long double from the convergent series and downward recursion.
+#pragma once
+
+#include "common.cuh"
+
+namespace jqc {
+
+template <typename T>
+struct BoysConst;
+template <>
+struct BoysConst<double> {
+  static constexpr int kTaylor = kBoysTaylor;
+};
+template <>
+struct BoysConst<float> {
+  static constexpr int kTaylor = kBoysTaylorF;
+};
+
+__device__ __forceinline__ double boys_exp(double x) { return exp(x); }
+__device__ __forceinline__ float boys_exp(float x) { return expf(x); }
+__device__ __forceinline__ double boys_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float boys_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ int boys_round(double x) { return __double2int_rn(x); }
+__device__ __forceinline__ int boys_round(float x) { return __float2int_rn(x); }
+
+// Writes F_0 .. F_M at T into F[0..M].  `tab` is the table for type T.
+template <typename T, int M>
+__device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tab, T (&F)[M + 1]) {
+  constexpr int KT = BoysConst<T>::kTaylor;
+  if (t < T(kBoysTMax)) {
+    const int i = boys_round(t * T(kBoysGridInv));
+    const T d = T(i) * T(1.0 / kBoysGridInv) - t;  // T_i - t
+    const T* row = tab + i * kBoysCols + M;
+    T acc = __ldg(row + KT - 1);
+#pragma unroll
+    for (int k = KT - 2; k >= 0; --k) acc = __ldg(row + k) + acc * (d * T(1.0 / (k + 1)));
+    F[M] = acc;
+    if (M > 0) {
+      const T e = boys_exp(-t);
+      const T t2 = t + t;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * T(1.0 / (2 * m + 1));
+    }
+  } else {
+    const T inv_t = T(1) / t;
+    F[0] = T(0.88622692545275801364908374167057) * boys_sqrt(inv_t);  // sqrt(pi)/2
+    if (M > 0) {
+      const T e = boys_exp(-t);
+      const T half_inv_t = T(0.5) * inv_t;
+#pragma unroll
+      for (int m = 0; m < M; ++m) F[m + 1] = (T(2 * m + 1) * F[m] - e) * half_inv_t;
+    }
+  }
+}
+
+// Runtime-order variant for the standalone Boys kernel (m <= kBoysMaxM).
+template <typename T>
+__device__ __forceinline__ void boys_eval_rt(T t, const T* __restrict__ tab, int M, T* F) {
+  constexpr int KT = BoysConst<T>::kTaylor;
+  if (t < T(kBoysTMax)) {
+    const int i = boys_round(t * T(kBoysGridInv));
+    const T d = T(i) * T(1.0 / kBoysGridInv) - t;
+    const T* row = tab + i * kBoysCols + M;
+    T acc = row[KT - 1];
+    for (int k = KT - 2; k >= 0; --k) acc = row[k] + acc * (d / T(k + 1));
+    F[M] = acc;
+    const T e = boys_exp(-t);
+    for (int m = M - 1; m >= 0; --m) F[m] = (T(2) * t * F[m + 1] + e) / T(2 * m + 1);
+  } else {
+    const T inv_t = T(1) / t;
+    F[0] = T(0.88622692545275801364908374167057) * boys_sqrt(inv_t);
+    const T e = boys_exp(-t);
+    for (int m = 0; m < M; ++m) F[m + 1] = (T(2 * m + 1) * F[m] - e) * T(0.5) * inv_t;
+  }
+}
+
+// Host: fill the FP64 table (kBoysRows * kBoysCols) in long double.
+void boys_fill_table(double* tab);
+
+// Per-device lazily created tables (device pointers).  The first call on a
+// device allocates and uploads them; later calls return the cached pointers.
+int boys_tables(int device, const double** d64, const float** d32);
+
+}  // namespace jqc

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 
 #include "../../include/jqc.h"
 
@@ -57,6 +58,17 @@ __host__ __device__ constexpr int cart_lz(int l, int k) { return l - cart_lx(l, 
 __host__ __device__ constexpr int herm_index(int t, int u, int v) {
   int s = t + u + v;
   return s * (s + 1) * (s + 2) / 6 + (s - t) * (s - t + 1) / 2 + (s - t - u);
+}
+
+// Compile-time loop: f(std::integral_constant<int, i>{}) for i = 0..N-1,
+// fully expanded by the front end (no reliance on the loop unroller).
+template <typename F, int... Is>
+__host__ __device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+  (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, typename F>
+__host__ __device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (N > 0) static_for_impl(f, std::make_integer_sequence<int, N>{});
 }
 
 }  // namespace jqc

@@ -1,0 +1,841 @@
+// Host side of libjqc.so: context, basis upload, shell-pair build with
+// Schwarz bounds, class-sorted work lists and the extern "C" entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace jqc {
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+#define JQC_REQUIRE(cond, code, msg) \
+  do {                               \
+    if (!(cond)) {                   \
+      set_error(msg);                \
+      return code;                   \
+    }                                \
+  } while (0)
+
+struct OneEParams {
+  int n_shell, n, n_atom;
+  const int* l;
+  const int* nprim;
+  const int* prim_off;
+  const double* exps;
+  const double* coefs;
+  const double* centres;
+  const int* ao;
+  const double* atom_xyz;
+  const double* atom_Z;
+  const double* boys;
+  double* S;
+  double* T;
+  double* V;
+};
+cudaError_t launch_one_e(const OneEParams& p, cudaStream_t s);
+
+cudaError_t fma_peak(bool fp32, int blocks, int iters, void* sink, cudaStream_t s, float* ms);
+cudaError_t launch_jk64_lo(int qc, const JKParams& p, cudaStream_t s);
+cudaError_t launch_jk64_hi(int qc, const JKParams& p, cudaStream_t s);
+cudaError_t launch_jk32_lo(int qc, const JKParams& p, cudaStream_t s);
+cudaError_t launch_jk32_hi(int qc, const JKParams& p, cudaStream_t s);
+cudaError_t launch_jk(int qc, bool fp32, const JKParams& p, cudaStream_t s) {
+  if (!is_reg_class(qc)) {
+    const int pb = qc_bra(qc), pk = qc_ket(qc);
+    return launch_warp_jk(pc_la(pb), pc_lb(pb), pc_la(pk), pc_lb(pk), fp32, p, s);
+  }
+  if (qc < 10) return fp32 ? launch_jk32_lo(qc, p, s) : launch_jk64_lo(qc, p, s);
+  return fp32 ? launch_jk32_hi(qc, p, s) : launch_jk64_hi(qc, p, s);
+}
+
+// ---------------------------------------------------------- device buffer
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  cudaError_t reserve(size_t count) {
+    if (count <= n && ptr) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&ptr, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  cudaError_t upload(const std::vector<T>& h, cudaStream_t s) {
+    cudaError_t e = reserve(h.size());
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpyAsync(ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  }
+};
+
+// ------------------------------------------------------------ Boys tables
+void boys_fill_table(double* tab) {
+  // F_m(T_i) by the convergent series e^{-T} sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1))
+  // at the top order, then downward recursion, all in long double.
+  const int top = kBoysCols - 1;
+  for (int i = 0; i < kBoysRows; ++i) {
+    const long double t = (long double)i / kBoysGridInv;
+    long double term = 1.0L / (2 * top + 1), sum = term;
+    for (int k = 1; k < 2000; ++k) {
+      term *= 2.0L * t / (2 * top + 2 * k + 1);
+      sum += term;
+      if (term < sum * 1e-22L) break;
+    }
+    long double e = expl(-t);
+    long double f = e * sum;
+    tab[i * kBoysCols + top] = (double)f;
+    for (int m = top - 1; m >= 0; --m) {
+      f = (2.0L * t * f + e) / (2 * m + 1);
+      tab[i * kBoysCols + m] = (double)f;
+    }
+  }
+}
+
+int boys_tables(int device, const double** d64, const float** d32) {
+  static std::mutex mu;
+  static std::vector<double*> t64;
+  static std::vector<float*> t32;
+  std::lock_guard<std::mutex> lock(mu);
+  int ndev = 0;
+  JQC_CUDA_CHECK(cudaGetDeviceCount(&ndev));
+  JQC_REQUIRE(device >= 0 && device < ndev, JQC_ERR_INVALID, "invalid CUDA device");
+  if ((int)t64.size() < ndev) {
+    t64.resize(ndev, nullptr);
+    t32.resize(ndev, nullptr);
+  }
+  if (!t64[device]) {
+    std::vector<double> h(kBoysRows * kBoysCols);
+    boys_fill_table(h.data());
+    std::vector<float> hf(h.begin(), h.end());
+    int prev = 0;
+    JQC_CUDA_CHECK(cudaGetDevice(&prev));
+    JQC_CUDA_CHECK(cudaSetDevice(device));
+    double* p64 = nullptr;
+    float* p32 = nullptr;
+    JQC_CUDA_CHECK(cudaMalloc(&p64, h.size() * sizeof(double)));
+    JQC_CUDA_CHECK(cudaMalloc(&p32, hf.size() * sizeof(float)));
+    JQC_CUDA_CHECK(cudaMemcpy(p64, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+    JQC_CUDA_CHECK(cudaMemcpy(p32, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    JQC_CUDA_CHECK(cudaSetDevice(prev));
+    t64[device] = p64;
+    t32[device] = p32;
+  }
+  *d64 = t64[device];
+  *d32 = t32[device];
+  return JQC_OK;
+}
+
+// ---------------------------------------------------------------- tasks
+struct TaskSet {
+  bool valid = false;
+  int mode = -1;
+  double mixed_tau = -1.0;
+  bool full = false;  // no quartet screening (dense tensor)
+  std::vector<Task> h;
+  DevBuf<Task> d;
+  int off[2][kNumQuartetClasses] = {};
+  int cnt[2][kNumQuartetClasses] = {};
+  long long n_quartets[2] = {0, 0};
+  long long n_prim_quartets = 0;
+  long long class_quartets[2][kNumQuartetClasses] = {};
+  long long class_prims[2][kNumQuartetClasses] = {};
+};
+
+struct Block {
+  int pc, ka, kb, start, count;
+};
+
+// Upper bound on primitive quartets one lane evaluates per task.
+constexpr int kMaxLanePrims = 256;
+constexpr int kNumStreams = 4;
+
+}  // namespace jqc
+
+using namespace jqc;
+
+struct jqc_ctx {
+  int device = 0;
+  // basis
+  int n_shell = 0, n_bf = 0, n_atom = 0;
+  std::vector<int> l, nprim, prim_off, ao, atom;
+  std::vector<double> exps, coefs, centres, atom_xyz, atom_Z;
+  DevBuf<double> d_centres;
+  DevBuf<int> d_ao, d_l, d_atom, d_nprim, d_prim_off;
+  DevBuf<double> d_atom_xyz, d_atom_Z, d_exps, d_coefs;
+  bool basis_ready = false;
+  // pairs (sorted: block by (class, K_a, K_b), Q descending inside)
+  bool pairs_ready = false;
+  double tau = 0.0;
+  long long n_pairs_all = 0;
+  std::vector<ShellPair> pairs;
+  std::vector<Block> blocks;
+  std::vector<double> Qmat;  // n_shell x n_shell, original order
+  DevBuf<ShellPair> d_pairs;
+  DevBuf<PrimPair> d_pp;
+  DevBuf<PrimPairF> d_ppf;
+  // work lists: one per (precision mode, mixed_tau) in use, plus the dense one
+  std::vector<TaskSet*> jk_cache;
+  TaskSet* jk_cur = nullptr;
+  TaskSet full_tasks;
+  // scratch
+  DevBuf<float> d_dmax;
+  cudaStream_t side[kNumStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kNumStreams] = {};
+  const double* boys64 = nullptr;
+  const float* boys32 = nullptr;
+};
+
+namespace jqc {
+
+static void make_prim_pairs(const jqc_ctx* c, int a, int b, std::vector<PrimPair>& out) {
+  const double* A = &c->centres[3 * a];
+  const double* B = &c->centres[3 * b];
+  const double dx = A[0] - B[0], dy = A[1] - B[1], dz = A[2] - B[2];
+  const double ab2 = dx * dx + dy * dy + dz * dz;
+  for (int i = 0; i < c->nprim[a]; ++i)
+    for (int j = 0; j < c->nprim[b]; ++j) {
+      const double al = c->exps[c->prim_off[a] + i], be = c->exps[c->prim_off[b] + j];
+      const double p = al + be;
+      PrimPair q;
+      q.p = p;
+      q.Px = (al * A[0] + be * B[0]) / p;
+      q.Py = (al * A[1] + be * B[1]) / p;
+      q.Pz = (al * A[2] + be * B[2]) / p;
+      q.K = std::exp(-(al * be / p) * ab2) * c->coefs[c->prim_off[a] + i] * c->coefs[c->prim_off[b] + j];
+      q.alpha = al;
+      q.beta = be;
+      q.pad = 0.0;
+      out.push_back(q);
+    }
+}
+
+// Number of leading entries k in [0, limit) of a Q-descending block with
+// Qi * Q[k] >= thr.
+static int prefix_count(const std::vector<ShellPair>& pairs, int start, int limit, double Qi, double thr) {
+  if (thr <= 0.0) return limit;
+  int lo = 0, hi = limit;
+  while (lo < hi) {
+    int mid = (lo + hi) / 2;
+    if (Qi * pairs[start + mid].Q >= thr)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s) {
+  std::vector<Task> lists[2][kNumQuartetClasses];
+  long long nq[2] = {0, 0}, npq = 0;
+  long long cq[2][kNumQuartetClasses] = {}, cp[2][kNumQuartetClasses] = {};
+  const double tau = full ? 0.0 : c->tau;
+  for (size_t cb = 0; cb < c->blocks.size(); ++cb) {
+    const Block& B = c->blocks[cb];
+    for (int pi = 0; pi < B.count; ++pi) {
+      const int gi = B.start + pi;
+      const double Qi = c->pairs[gi].Q;
+      for (size_t ck = 0; ck <= cb; ++ck) {
+        const Block& K = c->blocks[ck];
+        const int limit = (ck == cb) ? pi + 1 : K.count;
+        const int n_all = prefix_count(c->pairs, K.start, limit, Qi, tau);
+        int n64 = n_all;
+        if (mode == JQC_PREC_FP32) n64 = 0;
+        if (mode == JQC_PREC_MIXED) n64 = std::min(n_all, prefix_count(c->pairs, K.start, limit, Qi, mixed_tau));
+        const int qc = quartet_class(B.pc, K.pc);
+        const int seg[3] = {0, n64, n_all};
+        // Split the bra primitive pairs so one lane does at most ~kMaxLanePrims
+        // primitive quartets per task (the tensor keeps whole quartets).
+        const int nbp = c->pairs[gi].npp, nkp = K.ka * K.kb;
+        int chunk = nbp;
+        if (!full) chunk = std::max(1, std::min(nbp, kMaxLanePrims / std::max(1, nkp)));
+        // Register classes: 32 kets per warp task (one per lane).  Warp-engine
+        // classes: one ket per task, so every quartet gets its own warp.
+        const int per_task = is_reg_class(qc) ? 32 : 1;
+        for (int prec = 0; prec < 2; ++prec) {
+          for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
+            for (int b0 = 0; b0 < nbp; b0 += chunk) {
+              Task t;
+              t.bra = gi;
+              t.ket0 = K.start + k0;
+              t.nket = std::min(per_task, seg[prec + 1] - k0);
+              t.flags = b0 | (std::min(nbp, b0 + chunk) << 16);
+              lists[prec][qc].push_back(t);
+            }
+          }
+          nq[prec] += seg[prec + 1] - seg[prec];
+          cq[prec][qc] += seg[prec + 1] - seg[prec];
+          cp[prec][qc] += (long long)(seg[prec + 1] - seg[prec]) * nbp * nkp;
+        }
+        npq += (long long)n_all * c->pairs[gi].npp * K.ka * K.kb;
+      }
+    }
+  }
+  // Longest tasks first inside each class launch (cost = lane primitive quartets).
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      auto& v = lists[prec][qc];
+      std::stable_sort(v.begin(), v.end(), [&](const Task& x, const Task& y) {
+        const long long cx = (long long)((x.flags >> 16) - (x.flags & 0xffff)) * c->pairs[x.ket0].npp;
+        const long long cy = (long long)((y.flags >> 16) - (y.flags & 0xffff)) * c->pairs[y.ket0].npp;
+        return cx > cy;
+      });
+    }
+  ts.h.clear();
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      ts.off[prec][qc] = (int)ts.h.size();
+      ts.cnt[prec][qc] = (int)lists[prec][qc].size();
+      ts.h.insert(ts.h.end(), lists[prec][qc].begin(), lists[prec][qc].end());
+    }
+  JQC_CUDA_CHECK(ts.d.upload(ts.h, s));
+  ts.n_quartets[0] = nq[0];
+  ts.n_quartets[1] = nq[1];
+  ts.n_prim_quartets = npq;
+  std::memcpy(ts.class_quartets, cq, sizeof(cq));
+  std::memcpy(ts.class_prims, cp, sizeof(cp));
+  ts.mode = mode;
+  ts.mixed_tau = mixed_tau;
+  ts.full = full;
+  ts.valid = true;
+  return JQC_OK;
+}
+
+static int ensure_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s) {
+  if (mode != JQC_PREC_MIXED) mixed_tau = 0.0;
+  if (ts.valid && ts.mode == mode && ts.mixed_tau == mixed_tau && ts.full == full) return JQC_OK;
+  return build_tasks(c, ts, mode, mixed_tau, full, s);
+}
+
+// J/K work list for (mode, mixed_tau), built once and kept (a few per context).
+static int ensure_jk_tasks(jqc_ctx* c, int mode, double mixed_tau, cudaStream_t s) {
+  if (mode != JQC_PREC_MIXED) mixed_tau = 0.0;
+  for (TaskSet* ts : c->jk_cache)
+    if (ts->valid && ts->mode == mode && ts->mixed_tau == mixed_tau) {
+      c->jk_cur = ts;
+      return JQC_OK;
+    }
+  if (c->jk_cache.size() >= 4) {
+    delete c->jk_cache.front();
+    c->jk_cache.erase(c->jk_cache.begin());
+  }
+  TaskSet* ts = new TaskSet();
+  int rc = build_tasks(c, *ts, mode, mixed_tau, false, s);
+  if (rc) {
+    delete ts;
+    return rc;
+  }
+  c->jk_cache.push_back(ts);
+  c->jk_cur = ts;
+  return JQC_OK;
+}
+
+static void drop_jk_tasks(jqc_ctx* c) {
+  for (TaskSet* ts : c->jk_cache) delete ts;
+  c->jk_cache.clear();
+  c->jk_cur = nullptr;
+}
+
+static int select_device(const jqc_ctx* c) {
+  JQC_CUDA_CHECK(cudaSetDevice(c->device));
+  return JQC_OK;
+}
+
+}  // namespace jqc
+
+// ======================================================================
+// extern "C" API
+// ======================================================================
+extern "C" {
+
+const char* jqc_last_error(void) { return g_last_error.c_str(); }
+
+int jqc_version(void) { return 100; }
+
+int jqc_ctx_create(int device, jqc_ctx** out) {
+  JQC_REQUIRE(out != nullptr, JQC_ERR_INVALID, "jqc_ctx_create: out is null");
+  int ndev = 0;
+  JQC_CUDA_CHECK(cudaGetDeviceCount(&ndev));
+  JQC_REQUIRE(device >= 0 && device < ndev, JQC_ERR_INVALID, "jqc_ctx_create: invalid device");
+  jqc_ctx* c = new jqc_ctx();
+  c->device = device;
+  int rc = boys_tables(device, &c->boys64, &c->boys32);
+  if (rc != JQC_OK) {
+    delete c;
+    return rc;
+  }
+  cudaError_t e = cudaSetDevice(device);
+  for (int i = 0; i < kNumStreams && e == cudaSuccess; ++i) {
+    e = cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    set_error(std::string("jqc_ctx_create: ") + cudaGetErrorString(e));
+    jqc_ctx_destroy(c);
+    return JQC_ERR_CUDA;
+  }
+  *out = c;
+  return JQC_OK;
+}
+
+int jqc_ctx_destroy(jqc_ctx* ctx) {
+  if (ctx) {
+    cudaSetDevice(ctx->device);
+    for (int i = 0; i < kNumStreams; ++i) {
+      if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+      if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    drop_jk_tasks(ctx);
+    delete ctx;
+  }
+  return JQC_OK;
+}
+
+int jqc_basis_upload(jqc_ctx* c, int n_shell, const int* l, const int* nprim, const int* prim_off, const double* exps,
+                     const double* coefs, const double* centres, const int* atom_of_shell, int n_atom,
+                     const double* atom_xyz, const double* atom_charge, int cartesian) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_basis_upload: null context");
+  JQC_REQUIRE(n_shell > 0, JQC_ERR_INVALID, "jqc_basis_upload: n_shell must be positive");
+  JQC_REQUIRE(cartesian == 1, JQC_ERR_UNSUPPORTED, "jqc_basis_upload: only Cartesian shells are supported");
+  JQC_REQUIRE(l && nprim && prim_off && exps && coefs && centres && atom_of_shell, JQC_ERR_INVALID,
+              "jqc_basis_upload: null array");
+  JQC_REQUIRE(n_atom >= 0 && (n_atom == 0 || (atom_xyz && atom_charge)), JQC_ERR_INVALID,
+              "jqc_basis_upload: bad atom arrays");
+  int rc = select_device(c);
+  if (rc) return rc;
+  int np_total = 0;
+  for (int s = 0; s < n_shell; ++s) {
+    JQC_REQUIRE(l[s] >= 0, JQC_ERR_INVALID, "jqc_basis_upload: negative angular momentum");
+    JQC_REQUIRE(l[s] <= kMaxL, JQC_ERR_UNSUPPORTED, "jqc_basis_upload: angular momentum > 2 is not supported");
+    JQC_REQUIRE(nprim[s] > 0 && prim_off[s] >= 0, JQC_ERR_INVALID, "jqc_basis_upload: bad primitive range");
+    JQC_REQUIRE(atom_of_shell[s] >= 0 && (n_atom == 0 || atom_of_shell[s] < n_atom), JQC_ERR_INVALID,
+                "jqc_basis_upload: atom index out of range");
+    np_total = std::max(np_total, prim_off[s] + nprim[s]);
+  }
+  for (int i = 0; i < np_total; ++i) {
+    JQC_REQUIRE(std::isfinite(exps[i]) && exps[i] > 0.0, JQC_ERR_INVALID,
+                "jqc_basis_upload: exponents must be finite and positive");
+    JQC_REQUIRE(std::isfinite(coefs[i]), JQC_ERR_INVALID, "jqc_basis_upload: non-finite coefficient");
+  }
+  for (int i = 0; i < 3 * n_shell; ++i)
+    JQC_REQUIRE(std::isfinite(centres[i]), JQC_ERR_INVALID, "jqc_basis_upload: non-finite centre");
+  c->n_shell = n_shell;
+  c->l.assign(l, l + n_shell);
+  c->nprim.assign(nprim, nprim + n_shell);
+  c->prim_off.assign(prim_off, prim_off + n_shell);
+  c->exps.assign(exps, exps + np_total);
+  c->coefs.assign(coefs, coefs + np_total);
+  c->centres.assign(centres, centres + 3 * n_shell);
+  c->atom.assign(atom_of_shell, atom_of_shell + n_shell);
+  c->n_atom = n_atom;
+  c->atom_xyz.assign(atom_xyz ? atom_xyz : centres, atom_xyz ? atom_xyz + 3 * n_atom : centres);
+  c->atom_Z.assign(atom_charge ? atom_charge : centres, atom_charge ? atom_charge + n_atom : centres);
+  c->ao.resize(n_shell);
+  int off = 0;
+  for (int s = 0; s < n_shell; ++s) {
+    c->ao[s] = off;
+    off += ncart(l[s]);
+  }
+  c->n_bf = off;
+  cudaStream_t s0 = 0;
+  JQC_CUDA_CHECK(c->d_centres.upload(c->centres, s0));
+  JQC_CUDA_CHECK(c->d_ao.upload(c->ao, s0));
+  JQC_CUDA_CHECK(c->d_l.upload(c->l, s0));
+  JQC_CUDA_CHECK(c->d_atom.upload(c->atom, s0));
+  JQC_CUDA_CHECK(c->d_nprim.upload(c->nprim, s0));
+  JQC_CUDA_CHECK(c->d_prim_off.upload(c->prim_off, s0));
+  JQC_CUDA_CHECK(c->d_exps.upload(c->exps, s0));
+  JQC_CUDA_CHECK(c->d_coefs.upload(c->coefs, s0));
+  if (n_atom > 0) {
+    JQC_CUDA_CHECK(c->d_atom_xyz.upload(c->atom_xyz, s0));
+    JQC_CUDA_CHECK(c->d_atom_Z.upload(c->atom_Z, s0));
+  }
+  JQC_CUDA_CHECK(cudaStreamSynchronize(s0));
+  c->basis_ready = true;
+  c->pairs_ready = false;
+  drop_jk_tasks(c);
+  c->full_tasks.valid = false;
+  return JQC_OK;
+}
+
+int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_pairs_build: null context");
+  JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_pairs_build: call jqc_basis_upload first");
+  JQC_REQUIRE(schwarz_tau >= 0.0 && std::isfinite(schwarz_tau), JQC_ERR_INVALID,
+              "jqc_pairs_build: schwarz_tau must be >= 0");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // 1. all shell pairs a >= b (by l, then index), unsorted
+  std::vector<ShellPair> raw;
+  std::vector<PrimPair> rawpp;
+  std::vector<int> ids[kNumPairClasses];
+  for (int i = 0; i < c->n_shell; ++i)
+    for (int j = 0; j <= i; ++j) {
+      int a = i, b = j;
+      if (c->l[a] < c->l[b]) std::swap(a, b);
+      ShellPair sp;
+      sp.a = a;
+      sp.b = b;
+      sp.pp = (int)rawpp.size();
+      make_prim_pairs(c, a, b, rawpp);
+      sp.npp = (int)rawpp.size() - sp.pp;
+      sp.Q = 0.0;
+      sp.diag = (a == b);
+      sp.cls = pair_class(c->l[a], c->l[b]);
+      ids[sp.cls].push_back((int)raw.size());
+      raw.push_back(sp);
+    }
+  c->n_pairs_all = (long long)raw.size();
+  // 2. Schwarz bounds on the device
+  DevBuf<ShellPair> d_raw;
+  DevBuf<PrimPair> d_rawpp;
+  DevBuf<unsigned long long> d_q;
+  DevBuf<int> d_ids;
+  JQC_CUDA_CHECK(d_raw.upload(raw, s));
+  JQC_CUDA_CHECK(d_rawpp.upload(rawpp, s));
+  JQC_CUDA_CHECK(d_q.reserve(raw.size()));
+  JQC_CUDA_CHECK(cudaMemsetAsync(d_q.ptr, 0, raw.size() * sizeof(unsigned long long), s));
+  std::vector<int> all_ids;
+  int id_off[kNumPairClasses];
+  for (int pc = 0; pc < kNumPairClasses; ++pc) {
+    id_off[pc] = (int)all_ids.size();
+    all_ids.insert(all_ids.end(), ids[pc].begin(), ids[pc].end());
+  }
+  JQC_CUDA_CHECK(d_ids.upload(all_ids, s));
+  for (int pc = 0; pc < kNumPairClasses; ++pc) {
+    SchwarzParams p;
+    p.pair_ids = d_ids.ptr + id_off[pc];
+    p.n_pairs = (int)ids[pc].size();
+    p.pairs = d_raw.ptr;
+    p.pp = d_rawpp.ptr;
+    p.centres = c->d_centres.ptr;
+    p.boys = c->boys64;
+    p.qmax = d_q.ptr;
+    JQC_CUDA_CHECK(launch_schwarz(pc, p, s));
+  }
+  std::vector<unsigned long long> qbits(raw.size());
+  JQC_CUDA_CHECK(cudaMemcpyAsync(qbits.data(), d_q.ptr, qbits.size() * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+  JQC_CUDA_CHECK(cudaStreamSynchronize(s));
+  double qmax = 0.0;
+  c->Qmat.assign((size_t)c->n_shell * c->n_shell, 0.0);
+  for (size_t k = 0; k < raw.size(); ++k) {
+    double v;
+    std::memcpy(&v, &qbits[k], sizeof(double));
+    raw[k].Q = std::sqrt(std::max(v, 0.0));
+    qmax = std::max(qmax, raw[k].Q);
+    c->Qmat[(size_t)raw[k].a * c->n_shell + raw[k].b] = raw[k].Q;
+    c->Qmat[(size_t)raw[k].b * c->n_shell + raw[k].a] = raw[k].Q;
+  }
+  // 3. drop pairs that cannot pass, sort by (class, K_a, K_b) then Q desc
+  std::vector<int> keep;
+  for (size_t k = 0; k < raw.size(); ++k)
+    if (raw[k].Q * qmax >= schwarz_tau && raw[k].Q > 0.0) keep.push_back((int)k);
+  auto key = [&](int k) {
+    const ShellPair& p = raw[k];
+    return std::make_tuple(p.cls, c->nprim[p.a], c->nprim[p.b]);
+  };
+  std::stable_sort(keep.begin(), keep.end(), [&](int x, int y) {
+    auto kx = key(x), ky = key(y);
+    if (kx != ky) return kx < ky;
+    return raw[x].Q > raw[y].Q;
+  });
+  c->pairs.clear();
+  c->blocks.clear();
+  std::vector<PrimPair> pp;
+  std::vector<PrimPairF> ppf;
+  for (size_t r = 0; r < keep.size(); ++r) {
+    ShellPair sp = raw[keep[r]];
+    const int src = sp.pp;
+    sp.pp = (int)pp.size();
+    for (int k = 0; k < sp.npp; ++k) {
+      const PrimPair& q = rawpp[src + k];
+      pp.push_back(q);
+      ppf.push_back(PrimPairF{float(q.p), float(q.Px), float(q.Py), float(q.Pz), float(q.K), float(q.alpha),
+                              float(q.beta), 0.f});
+    }
+    auto kk = key(keep[r]);
+    if (c->blocks.empty() || std::get<0>(kk) != c->blocks.back().pc || std::get<1>(kk) != c->blocks.back().ka ||
+        std::get<2>(kk) != c->blocks.back().kb) {
+      c->blocks.push_back(Block{std::get<0>(kk), std::get<1>(kk), std::get<2>(kk), (int)c->pairs.size(), 0});
+    }
+    c->blocks.back().count++;
+    c->pairs.push_back(sp);
+  }
+  JQC_CUDA_CHECK(c->d_pairs.upload(c->pairs, s));
+  JQC_CUDA_CHECK(c->d_pp.upload(pp, s));
+  JQC_CUDA_CHECK(c->d_ppf.upload(ppf, s));
+  JQC_CUDA_CHECK(cudaStreamSynchronize(s));
+  c->tau = schwarz_tau;
+  c->pairs_ready = true;
+  drop_jk_tasks(c);
+  c->full_tasks.valid = false;
+  return JQC_OK;
+}
+
+int jqc_stats(jqc_ctx* c, int precision_mode, double mixed_tau, long long* out) {
+  JQC_REQUIRE(c && out, JQC_ERR_INVALID, "jqc_stats: null argument");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_stats: call jqc_pairs_build first");
+  JQC_REQUIRE(precision_mode >= 0 && precision_mode <= 2, JQC_ERR_INVALID, "jqc_stats: bad precision_mode");
+  int rc = select_device(c);
+  if (rc) return rc;
+  rc = ensure_jk_tasks(c, precision_mode, mixed_tau, 0);
+  if (rc) return rc;
+  JQC_CUDA_CHECK(cudaStreamSynchronize(0));
+  out[0] = c->n_pairs_all;
+  out[1] = (long long)c->pairs.size();
+  out[2] = c->jk_cur->n_quartets[0];
+  out[3] = c->jk_cur->n_quartets[1];
+  out[4] = c->jk_cur->n_prim_quartets;
+  out[5] = c->n_bf;
+  int launches = 2;  // J and K symmetrization
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) launches += c->jk_cur->cnt[prec][qc] > 0;
+  out[6] = (long long)c->jk_cur->h.size();
+  out[7] = launches;
+  return JQC_OK;
+}
+
+int jqc_class_stats(jqc_ctx* c, int precision_mode, double mixed_tau, long long* out) {
+  JQC_REQUIRE(c && out, JQC_ERR_INVALID, "jqc_class_stats: null argument");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_class_stats: call jqc_pairs_build first");
+  JQC_REQUIRE(precision_mode >= 0 && precision_mode <= 2, JQC_ERR_INVALID, "jqc_class_stats: bad precision_mode");
+  int rc = select_device(c);
+  if (rc) return rc;
+  rc = ensure_jk_tasks(c, precision_mode, mixed_tau, 0);
+  if (rc) return rc;
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      const int k = (prec * kNumQuartetClasses + qc) * 3;
+      out[k] = c->jk_cur->class_quartets[prec][qc];
+      out[k + 1] = c->jk_cur->class_prims[prec][qc];
+      out[k + 2] = c->jk_cur->cnt[prec][qc];
+    }
+  return JQC_OK;
+}
+
+int jqc_fp_peak(int fp32, int blocks, int iters, double* tflops, void* stream) {
+  JQC_REQUIRE(tflops != nullptr && blocks > 0 && iters > 0, JQC_ERR_INVALID, "jqc_fp_peak: bad argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  void* sink = nullptr;
+  JQC_CUDA_CHECK(cudaMalloc(&sink, (size_t)blocks * 8));
+  float ms = 0.f;
+  cudaError_t e = fma_peak(fp32 != 0, blocks, iters, sink, s, &ms);
+  cudaFree(sink);
+  JQC_CUDA_CHECK(e);
+  const double flops = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return JQC_OK;
+}
+
+int jqc_schwarz(jqc_ctx* c, double* Q, void* stream) {
+  JQC_REQUIRE(c && Q, JQC_ERR_INVALID, "jqc_schwarz: null argument");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_schwarz: call jqc_pairs_build first");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  JQC_CUDA_CHECK(cudaMemcpyAsync(Q, c->Qmat.data(), c->Qmat.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  JQC_CUDA_CHECK(cudaStreamSynchronize(s));
+  return JQC_OK;
+}
+
+int jqc_boys(const double* T, long long n, int mmax, void* out, int fp32, void* stream) {
+  JQC_REQUIRE(n >= 0, JQC_ERR_INVALID, "jqc_boys: n must be >= 0");
+  JQC_REQUIRE(mmax >= 0 && mmax <= kBoysMaxM, JQC_ERR_INVALID, "jqc_boys: mmax must be in [0, 16]");
+  if (n == 0) return JQC_OK;
+  JQC_REQUIRE(T && out, JQC_ERR_INVALID, "jqc_boys: null pointer");
+  int dev = 0;
+  JQC_CUDA_CHECK(cudaGetDevice(&dev));
+  const double* t64;
+  const float* t32;
+  int rc = boys_tables(dev, &t64, &t32);
+  if (rc) return rc;
+  JQC_CUDA_CHECK(launch_boys(T, n, mmax, out, fp32 != 0, fp32 ? (const void*)t32 : (const void*)t64,
+                             static_cast<cudaStream_t>(stream)));
+  return JQC_OK;
+}
+
+int jqc_eri_prim_quartets(int la, int lb, int lc, int ld, long long n, const double* exps, const double* centres,
+                          double* out, void* stream) {
+  JQC_REQUIRE(n >= 0, JQC_ERR_INVALID, "jqc_eri_prim_quartets: n must be >= 0");
+  JQC_REQUIRE(la >= 0 && lb >= 0 && lc >= 0 && ld >= 0, JQC_ERR_INVALID, "jqc_eri_prim_quartets: negative l");
+  JQC_REQUIRE(la <= kMaxL && lb <= kMaxL && lc <= kMaxL && ld <= kMaxL, JQC_ERR_UNSUPPORTED,
+              "jqc_eri_prim_quartets: l > 2 is not supported");
+  JQC_REQUIRE(la >= lb && lc >= ld && pair_class(la, lb) >= pair_class(lc, ld), JQC_ERR_UNSUPPORTED,
+              "jqc_eri_prim_quartets: class must satisfy la>=lb, lc>=ld, (la,lb)>=(lc,ld)");
+  if (n == 0) return JQC_OK;
+  JQC_REQUIRE(exps && centres && out, JQC_ERR_INVALID, "jqc_eri_prim_quartets: null pointer");
+  int dev = 0;
+  JQC_CUDA_CHECK(cudaGetDevice(&dev));
+  const double* t64;
+  const float* t32;
+  int rc = boys_tables(dev, &t64, &t32);
+  if (rc) return rc;
+  PrimQuartetParams p{n, exps, centres, t64, out};
+  JQC_CUDA_CHECK(launch_prim_quartets(la, lb, lc, ld, p, static_cast<cudaStream_t>(stream)));
+  return JQC_OK;
+}
+
+int jqc_eri_tensor(jqc_ctx* c, double* out, long long max_bytes, void* stream) {
+  JQC_REQUIRE(c && out, JQC_ERR_INVALID, "jqc_eri_tensor: null argument");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_eri_tensor: call jqc_pairs_build first");
+  const double bytes = std::pow((double)c->n_bf, 4) * 8.0;
+  JQC_REQUIRE(bytes <= (double)max_bytes, JQC_ERR_TOO_LARGE,
+              "jqc_eri_tensor: n^4 tensor exceeds max_bytes; use jqc_jk (direct J/K) instead");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  rc = ensure_tasks(c, c->full_tasks, JQC_PREC_FP64, 0.0, true, s);
+  if (rc) return rc;
+  JQC_CUDA_CHECK(cudaMemsetAsync(out, 0, (size_t)bytes, s));
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    TensorParams p;
+    p.tasks = c->full_tasks.d.ptr + c->full_tasks.off[0][qc];
+    p.n_tasks = c->full_tasks.cnt[0][qc];
+    p.pairs = c->d_pairs.ptr;
+    p.pp = c->d_pp.ptr;
+    p.centres = c->d_centres.ptr;
+    p.ao = c->d_ao.ptr;
+    p.boys = c->boys64;
+    p.eri = out;
+    p.n = c->n_bf;
+    JQC_CUDA_CHECK(launch_eri_tensor(qc, p, s));
+  }
+  return JQC_OK;
+}
+
+int jqc_one_electron(jqc_ctx* c, double* S, double* T, double* V, void* stream) {
+  JQC_REQUIRE(c && S && T && V, JQC_ERR_INVALID, "jqc_one_electron: null argument");
+  JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_one_electron: call jqc_basis_upload first");
+  int rc = select_device(c);
+  if (rc) return rc;
+  OneEParams p;
+  p.n_shell = c->n_shell;
+  p.n = c->n_bf;
+  p.n_atom = c->n_atom;
+  p.l = c->d_l.ptr;
+  p.nprim = c->d_nprim.ptr;
+  p.prim_off = c->d_prim_off.ptr;
+  p.exps = c->d_exps.ptr;
+  p.coefs = c->d_coefs.ptr;
+  p.centres = c->d_centres.ptr;
+  p.ao = c->d_ao.ptr;
+  p.atom_xyz = c->d_atom_xyz.ptr;
+  p.atom_Z = c->d_atom_Z.ptr;
+  p.boys = c->boys64;
+  p.S = S;
+  p.T = T;
+  p.V = V;
+  JQC_CUDA_CHECK(launch_one_e(p, static_cast<cudaStream_t>(stream)));
+  return JQC_OK;
+}
+
+static int jk_impl(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, int precision_mode,
+                   double mixed_tau, double dens_tau, cudaStream_t s, double* class_ms);
+
+int jqc_jk_timed(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, int precision_mode, double mixed_tau,
+                 double dens_tau, void* stream, double* class_ms) {
+  JQC_REQUIRE(class_ms != nullptr, JQC_ERR_INVALID, "jqc_jk_timed: class_ms is null");
+  return jk_impl(c, n_dens, D, J, K, precision_mode, mixed_tau, dens_tau, static_cast<cudaStream_t>(stream),
+                 class_ms);
+}
+
+int jqc_jk(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, int precision_mode, double mixed_tau,
+           double dens_tau, void* stream) {
+  return jk_impl(c, n_dens, D, J, K, precision_mode, mixed_tau, dens_tau, static_cast<cudaStream_t>(stream),
+                 nullptr);
+}
+
+static int jk_impl(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, int precision_mode,
+                   double mixed_tau, double dens_tau, cudaStream_t s, double* class_ms) {
+  JQC_REQUIRE(c && D && J && K, JQC_ERR_INVALID, "jqc_jk: null argument");
+  JQC_REQUIRE(n_dens >= 1 && n_dens <= 4, JQC_ERR_INVALID, "jqc_jk: n_dens must be 1..4");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_jk: call jqc_pairs_build first");
+  JQC_REQUIRE(precision_mode >= 0 && precision_mode <= 2, JQC_ERR_INVALID, "jqc_jk: bad precision_mode");
+  JQC_REQUIRE(mixed_tau >= 0.0 && dens_tau >= 0.0, JQC_ERR_INVALID, "jqc_jk: thresholds must be >= 0");
+  int rc = select_device(c);
+  if (rc) return rc;
+  rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+  if (rc) return rc;
+  const int n = c->n_bf;
+  const size_t nn = (size_t)n * n * n_dens;
+  JQC_CUDA_CHECK(cudaMemsetAsync(J, 0, nn * sizeof(double), s));
+  JQC_CUDA_CHECK(cudaMemsetAsync(K, 0, nn * sizeof(double), s));
+  if (class_ms)
+    for (int k = 0; k < 2 * kNumQuartetClasses; ++k) class_ms[k] = 0.0;
+  const float* dmax = nullptr;
+  if (dens_tau > 0.0) {
+    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
+    JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, c->d_dmax.ptr, s));
+    dmax = c->d_dmax.ptr;
+  }
+  // Class kernels run concurrently on the context's side streams (they only
+  // add into J/K with atomics), forked from and joined back into `stream`.
+  JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
+  for (int i = 0; i < kNumStreams; ++i) JQC_CUDA_CHECK(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
+  int li = 0;
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      JKParams p;
+      p.tasks = c->jk_cur->d.ptr + c->jk_cur->off[prec][qc];
+      p.n_tasks = c->jk_cur->cnt[prec][qc];
+      if (p.n_tasks == 0) continue;
+      p.pairs = c->d_pairs.ptr;
+      p.pp = prec ? (const void*)c->d_ppf.ptr : (const void*)c->d_pp.ptr;
+      p.centres = c->d_centres.ptr;
+      p.ao = c->d_ao.ptr;
+      p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
+      p.D = D;
+      p.J = J;
+      p.K = K;
+      p.n = n;
+      p.n_dens = n_dens;
+      p.dmax = dmax;
+      p.n_shell = c->n_shell;
+      p.dens_tau = (float)dens_tau;
+      if (class_ms) {
+        cudaEvent_t e0, e1;
+        JQC_CUDA_CHECK(cudaEventCreate(&e0));
+        JQC_CUDA_CHECK(cudaEventCreate(&e1));
+        JQC_CUDA_CHECK(cudaEventRecord(e0, s));
+        JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, s));
+        JQC_CUDA_CHECK(cudaEventRecord(e1, s));
+        JQC_CUDA_CHECK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        JQC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+        class_ms[prec * kNumQuartetClasses + qc] = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+      } else {
+        JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, c->side[li++ % kNumStreams]));
+      }
+    }
+  for (int i = 0; i < kNumStreams; ++i) {
+    JQC_CUDA_CHECK(cudaEventRecord(c->ev_join[i], c->side[i]));
+    JQC_CUDA_CHECK(cudaStreamWaitEvent(s, c->ev_join[i], 0));
+  }
+  JQC_CUDA_CHECK(launch_symmetrize(J, n_dens, n, s));
+  JQC_CUDA_CHECK(launch_symmetrize(K, n_dens, n, s));
+  return JQC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,214 @@
+// ERI-tensor, Schwarz, primitive-quartet and Boys kernels plus small helpers.
+#include "jk_impl.cuh"
+
+namespace jqc {
+
+// ----------------------------------------------------------------- Schwarz
+// screening.py:32-58: Q_ab = sqrt(max over Cartesian ab of (ab|ab)).
+template <int LA, int LB, int NS>
+struct SchwarzBody {
+  const SchwarzParams& prm;
+  int pid;
+
+  template <int PART>
+  __device__ __forceinline__ void run() {
+    using Cfg = QCfg<LA, LB, LA, LB, NS, PART>;
+    if constexpr (Cfg::NCDP > 0) body<PART>();
+  }
+
+  template <int PART>
+  __device__ __forceinline__ void body() {
+    using Cfg = QCfg<LA, LB, LA, LB, NS, PART>;
+    const int id = prm.pair_ids[pid];
+    const ShellPair bp = prm.pairs[id];
+    const double* ctr = prm.centres;
+    Vec3<double> A{ctr[3 * bp.a], ctr[3 * bp.a + 1], ctr[3 * bp.a + 2]};
+    Vec3<double> B{ctr[3 * bp.b], ctr[3 * bp.b + 1], ctr[3 * bp.b + 2]};
+    double out[Cfg::NAB][Cfg::CDP];
+    double ebuf[3][LA + 1][LB + 1][LA + LB + 1];
+    quartet_accumulate<double, LA, LB, LA, LB, NS, PART, false>(prm.pp + bp.pp, bp.npp, A, B, prm.pp + bp.pp,
+                                                                 bp.npp, A, B, prm.boys, ebuf, out);
+    double m = 0.0;
+    static_for<Cfg::NCDP>([&](auto c_) {
+      constexpr int cdi = decltype(c_)::value;
+      m = fmax(m, out[Cfg::CD0 + cdi][cdi]);
+    });
+    atomicMax(prm.qmax + id, (unsigned long long)__double_as_longlong(m));
+  }
+};
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(128) schwarz_kernel(const SchwarzParams prm) {
+  constexpr int NS = class_split(LA, LB, LA, LB);
+  const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pid >= prm.n_pairs) return;
+  SchwarzBody<LA, LB, NS> body{prm, pid};
+  dispatch_part<NS>(blockIdx.y, body);
+}
+
+cudaError_t launch_schwarz(int pc, const SchwarzParams& p, cudaStream_t s) {
+  if (p.n_pairs == 0) return cudaSuccess;
+  if (!is_reg_class(quartet_class(pc, pc))) return launch_warp_schwarz(pc_la(pc), pc_lb(pc), p, s);
+  switch (pc) {
+#define S(PC, A, B)                                                       \
+  case PC: {                                                              \
+    dim3 grid((p.n_pairs + 127) / 128, class_split(A, B, A, B));          \
+    schwarz_kernel<A, B><<<grid, 128, 0, s>>>(p);                         \
+    return cudaGetLastError();                                            \
+  }
+    S(0, 0, 0) S(1, 1, 0) S(2, 1, 1) S(3, 2, 0) S(4, 2, 1)
+#undef S
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+// --------------------------------------------------------- primitive blocks
+// obara_saika.py:227-332 primitive_eri_block for a batch of primitive
+// quartets with unit coefficients (K_AB and K_CD included).
+template <int LA, int LB, int LC, int LD, int NS>
+struct PrimBody {
+  const PrimQuartetParams& prm;
+  long long q;
+
+  template <int PART>
+  __device__ __forceinline__ void run() {
+    using Cfg = QCfg<LA, LB, LC, LD, NS, PART>;
+    if constexpr (Cfg::NCDP > 0) body<PART>();
+  }
+
+  template <int PART>
+  __device__ __forceinline__ void body() {
+    using Cfg = QCfg<LA, LB, LC, LD, NS, PART>;
+    const double* ex = prm.exps + 4 * q;
+    const double* c = prm.centres + 12 * q;
+    Vec3<double> A{c[0], c[1], c[2]}, B{c[3], c[4], c[5]}, C{c[6], c[7], c[8]}, D{c[9], c[10], c[11]};
+    PrimPair bra, ket;
+    {
+      const double al = ex[0], be = ex[1], p = al + be;
+      const double dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
+      bra = PrimPair{p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
+                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.0};
+    }
+    {
+      const double al = ex[2], be = ex[3], p = al + be;
+      const double dx = C.x - D.x, dy = C.y - D.y, dz = C.z - D.z;
+      ket = PrimPair{p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
+                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.0};
+    }
+    double out[Cfg::NAB][Cfg::CDP];
+    double ebuf[3][LA + 1][LB + 1][LA + LB + 1];
+    quartet_accumulate<double, LA, LB, LC, LD, NS, PART, false>(&bra, 1, A, B, &ket, 1, C, D, prm.boys, ebuf, out);
+    double* o = prm.out + q * (Cfg::NAB * Cfg::NCD);
+    static_for<Cfg::NAB * Cfg::NCDP>([&](auto x_) {
+      constexpr int x = decltype(x_)::value;
+      constexpr int ab = x / Cfg::NCDP, cdi = x % Cfg::NCDP;
+      o[ab * Cfg::NCD + Cfg::CD0 + cdi] = out[ab][cdi];
+    });
+  }
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) prim_kernel(const PrimQuartetParams prm) {
+  constexpr int NS = class_split(LA, LB, LC, LD);
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= prm.n) return;
+  PrimBody<LA, LB, LC, LD, NS> body{prm, q};
+  dispatch_part<NS>(blockIdx.y, body);
+}
+
+cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s) {
+  if (p.n == 0) return cudaSuccess;
+  if (la < lb || lc < ld || la > 2 || lc > 2) return cudaErrorInvalidValue;
+  const int pb = pair_class(la, lb), pk = pair_class(lc, ld);
+  if (pb < pk) return cudaErrorInvalidValue;
+  const unsigned gx = (unsigned)((p.n + 127) / 128);
+  if (!is_reg_class(quartet_class(pb, pk))) return launch_warp_prim(la, lb, lc, ld, p, s);
+  switch (quartet_class(pb, pk)) {
+#define X(Q, A, B, C, D)                                                                     \
+  case Q: {                                                                                  \
+    dim3 grid(gx, class_split(A, B, C, D));                                                  \
+    prim_kernel<A, B, C, D><<<grid, 128, 0, s>>>(p);                                         \
+    return cudaGetLastError();                                                               \
+  }
+    JQC_FOR_REG_CLASSES(X)
+#undef X
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+// -------------------------------------------------------------------- Boys
+template <typename T>
+__global__ void boys_kernel(const double* __restrict__ tv, long long n, int mmax, T* __restrict__ out,
+                            const T* __restrict__ tab) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double t = tv[i];
+  if (!(t >= 0.0)) {  // negative or NaN argument: no table access
+    for (int m = 0; m <= mmax; ++m) out[i * (mmax + 1) + m] = T(NAN);
+    return;
+  }
+  T F[kBoysMaxM + 1];
+  boys_eval_rt<T>(T(t), tab, mmax, F);
+  for (int m = 0; m <= mmax; ++m) out[i * (mmax + 1) + m] = F[m];
+}
+
+cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tab,
+                        cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const unsigned g = (unsigned)((n + 255) / 256);
+  if (fp32)
+    boys_kernel<float><<<g, 256, 0, s>>>(T, n, mmax, static_cast<float*>(out), static_cast<const float*>(tab));
+  else
+    boys_kernel<double><<<g, 256, 0, s>>>(T, n, mmax, static_cast<double*>(out), static_cast<const double*>(tab));
+  return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- helpers
+__global__ void dmax_kernel(const double* __restrict__ D, int n_dens, int n, int n_shell, const int* __restrict__ ao,
+                            const int* __restrict__ l, float* __restrict__ dmax) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_shell * n_shell) return;
+  const int i = idx / n_shell, j = idx % n_shell;
+  const int ni = ncart(l[i]), nj = ncart(l[j]);
+  double m = 0.0;
+  for (int d = 0; d < n_dens; ++d)
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nj; ++b) m = fmax(m, fabs(D[(size_t)d * n * n + (size_t)(ao[i] + a) * n + ao[j] + b]));
+  dmax[idx] = float(m);
+}
+
+cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
+                        cudaStream_t s) {
+  const int tot = n_shell * n_shell;
+  dmax_kernel<<<(tot + 255) / 256, 256, 0, s>>>(D, n_dens, n, n_shell, ao, l, dmax);
+  return cudaGetLastError();
+}
+
+// M <- M + M^T for `count` consecutive n x n matrices.
+__global__ void symmetrize_kernel(double* M, int count, int n) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nn = (long long)n * n;
+  if (idx >= nn * count) return;
+  const int m = int(idx / nn);
+  const int i = int((idx % nn) / n), j = int(idx % n);
+  if (i < j) return;
+  double* A = M + m * nn;
+  if (i == j) {
+    A[(size_t)i * n + i] *= 2.0;
+  } else {
+    const double v = A[(size_t)i * n + j] + A[(size_t)j * n + i];
+    A[(size_t)i * n + j] = v;
+    A[(size_t)j * n + i] = v;
+  }
+}
+
+cudaError_t launch_symmetrize(double* M, int count, int n, cudaStream_t s) {
+  const long long tot = (long long)n * n * count;
+  if (tot == 0) return cudaSuccess;
+  symmetrize_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(M, count, n);
+  return cudaGetLastError();
+}
+
+}  // namespace jqc

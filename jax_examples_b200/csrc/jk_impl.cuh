@@ -1,0 +1,228 @@
+// Fused ERI + J/K digestion kernel (one template per angular class).
+//
+// Work mapping: one warp takes one Task = one bra shell pair against up to 32
+// consecutive ket shell pairs of one (class, contraction) block; lane i owns
+// ket pair ket0+i.  blockIdx.y selects the part of the ket Cartesian pairs a
+// thread computes (classes with many components are split so the block fits
+// in registers).  The contracted integral block never leaves registers: it is
+// contracted with D on the spot and added to J and K.
+//
+// Digestion (fock.py:31-38 restated with 8-fold symmetry): for a canonical
+// quartet with scale s = 1/2 per coincidence (a==b shell, c==d shell,
+// bra pair == ket pair), every element v = (ab|cd) adds
+//   J[a][b] += 2 s v D[c][d],  J[c][d] += 2 s v D[a][b]
+//   K[a][d] += s v D[c][b], K[b][d] += s v D[c][a],
+//   K[a][c] += s v D[d][b], K[b][c] += s v D[d][a]
+// into accumulators A (J) and B (K); afterwards J = A + A^T, K = B + B^T.
+// J[a][b] is summed over the warp with shuffles before one atomic per
+// element; everything else goes to FP64 atomics directly.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace jqc {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T, int LA, int LB, int LC, int LD, int NS>
+struct JKBody {
+  const JKParams& prm;
+  int warp;
+  int lane;
+  T (*ebra)[LA + 1][LB + 1][LA + LB + 1];  // warp-private shared memory
+
+  template <int PART>
+  __device__ __forceinline__ void run() {
+    using Cfg = QCfg<LA, LB, LC, LD, NS, PART>;
+    if constexpr (Cfg::NCDP > 0) body<PART>();
+  }
+
+  template <int PART>
+  __device__ __forceinline__ void body() {
+    using Cfg = QCfg<LA, LB, LC, LD, NS, PART>;
+    using PPT = typename PPType<T>::type;
+    constexpr int NA = Cfg::NA, NB = Cfg::NB, ND = Cfg::ND;
+    constexpr int NCDP = Cfg::NCDP;
+
+    const Task task = prm.tasks[warp];
+    const ShellPair bp = prm.pairs[task.bra];
+    const bool in_range = lane < task.nket;
+    const int kidx = task.ket0 + (in_range ? lane : 0);
+    const ShellPair kp = prm.pairs[kidx];
+    bool active = in_range;
+    if (prm.dmax != nullptr && active) {
+      const float* dm = prm.dmax;
+      const int ns = prm.n_shell;
+      float m = fmaxf(2.f * dm[bp.a * ns + bp.b], 2.f * dm[kp.a * ns + kp.b]);
+      m = fmaxf(m, fmaxf(dm[bp.a * ns + kp.a], dm[bp.a * ns + kp.b]));
+      m = fmaxf(m, fmaxf(dm[bp.b * ns + kp.a], dm[bp.b * ns + kp.b]));
+      if (float(bp.Q) * float(kp.Q) * m < prm.dens_tau) active = false;
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0u) return;
+
+    const PPT* pp = static_cast<const PPT*>(prm.pp);
+    const double* ctr = prm.centres;
+    Vec3<T> A{T(ctr[3 * bp.a]), T(ctr[3 * bp.a + 1]), T(ctr[3 * bp.a + 2])};
+    Vec3<T> B{T(ctr[3 * bp.b]), T(ctr[3 * bp.b + 1]), T(ctr[3 * bp.b + 2])};
+    Vec3<T> C{T(ctr[3 * kp.a]), T(ctr[3 * kp.a + 1]), T(ctr[3 * kp.a + 2])};
+    Vec3<T> D{T(ctr[3 * kp.b]), T(ctr[3 * kp.b + 1]), T(ctr[3 * kp.b + 2])};
+
+    T out[Cfg::NAB][Cfg::CDP];
+    const int p0 = task.flags & 0xffff, p1 = task.flags >> 16;  // bra primitive-pair range
+    quartet_accumulate<T, LA, LB, LC, LD, NS, PART, true>(pp + bp.pp + p0, p1 - p0, A, B, pp + kp.pp,
+                                                           active ? kp.npp : 0, C, D, static_cast<const T*>(prm.boys),
+                                                           ebra, out);
+
+    double s = active ? 1.0 : 0.0;
+    if (bp.diag) s *= 0.5;
+    if (kp.diag) s *= 0.5;
+    if (task.bra == kidx) s *= 0.5;
+
+    const int n = prm.n;
+    const int a0 = prm.ao[bp.a], b0 = prm.ao[bp.b], c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];
+    for (int dd = 0; dd < prm.n_dens; ++dd) {
+      const double* Dm = prm.D + (size_t)dd * n * n;
+      double* Jm = prm.J + (size_t)dd * n * n;
+      double* Km = prm.K + (size_t)dd * n * n;
+      // J[a][b] (warp-uniform target): reduce over lanes first.
+      double dcd[NCDP];
+      static_for<NCDP>([&](auto cdi_) {
+        constexpr int cdi = decltype(cdi_)::value;
+        constexpr int cd = Cfg::CD0 + cdi, c = cd / ND, d = cd % ND;
+        dcd[cdi] = active ? __ldg(Dm + (size_t)(c0 + c) * n + d0 + d) : 0.0;
+      });
+      static_for<NA * NB>([&](auto ab_) {
+        constexpr int ab = decltype(ab_)::value;
+        double acc = 0.0;
+        static_for<NCDP>([&](auto cdi_) {
+          constexpr int cdi = decltype(cdi_)::value;
+          acc += double(out[ab][cdi]) * dcd[cdi];
+        });
+        acc = warp_sum(2.0 * s * acc);
+        if (lane == 0) atomicAdd(Jm + (size_t)(a0 + ab / NB) * n + b0 + ab % NB, acc);
+      });
+      if (!active) continue;
+      // J[c][d]
+      double dab[NA * NB];
+      static_for<NA * NB>([&](auto ab_) {
+        constexpr int ab = decltype(ab_)::value;
+        dab[ab] = __ldg(Dm + (size_t)(a0 + ab / NB) * n + b0 + ab % NB);
+      });
+      static_for<NCDP>([&](auto cdi_) {
+        constexpr int cdi = decltype(cdi_)::value;
+        constexpr int cd = Cfg::CD0 + cdi, c = cd / ND, d = cd % ND;
+        double acc = 0.0;
+        static_for<NA * NB>([&](auto ab_) {
+          constexpr int ab = decltype(ab_)::value;
+          acc += double(out[ab][cdi]) * dab[ab];
+        });
+        atomicAdd(Jm + (size_t)(c0 + c) * n + d0 + d, 2.0 * s * acc);
+      });
+      // K: four blocks, for the (c, d) of this part.
+      static_for<NCDP>([&](auto cdi_) {
+        constexpr int cdi = decltype(cdi_)::value;
+        constexpr int cd = Cfg::CD0 + cdi, c = cd / ND, d = cd % ND;
+        // K[a][d] += sum_b v D[c][b];  K[a][c] += sum_b v D[d][b]
+        static_for<NA>([&](auto a_) {
+          constexpr int a = decltype(a_)::value;
+          double kad = 0.0, kac = 0.0;
+          static_for<NB>([&](auto b_) {
+            constexpr int b = decltype(b_)::value;
+            const double v = double(out[a * NB + b][cdi]);
+            kad += v * __ldg(Dm + (size_t)(c0 + c) * n + b0 + b);
+            kac += v * __ldg(Dm + (size_t)(d0 + d) * n + b0 + b);
+          });
+          atomicAdd(Km + (size_t)(a0 + a) * n + d0 + d, s * kad);
+          atomicAdd(Km + (size_t)(a0 + a) * n + c0 + c, s * kac);
+        });
+        // K[b][d] += sum_a v D[c][a];  K[b][c] += sum_a v D[d][a]
+        static_for<NB>([&](auto b_) {
+          constexpr int b = decltype(b_)::value;
+          double kbd = 0.0, kbc = 0.0;
+          static_for<NA>([&](auto a_) {
+            constexpr int a = decltype(a_)::value;
+            const double v = double(out[a * NB + b][cdi]);
+            kbd += v * __ldg(Dm + (size_t)(c0 + c) * n + a0 + a);
+            kbc += v * __ldg(Dm + (size_t)(d0 + d) * n + a0 + a);
+          });
+          atomicAdd(Km + (size_t)(b0 + b) * n + d0 + d, s * kbd);
+          atomicAdd(Km + (size_t)(b0 + b) * n + c0 + c, s * kbc);
+        });
+      });
+    }
+  }
+};
+
+template <typename T, int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) jk_kernel(const JKParams prm) {
+  constexpr int NS = class_split(LA, LB, LC, LD);
+  __shared__ T sE[4][3][LA + 1][LB + 1][LA + LB + 1];
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp >= prm.n_tasks) return;
+  JKBody<T, LA, LB, LC, LD, NS> body{prm, warp, int(threadIdx.x & 31), sE[threadIdx.x >> 5]};
+  dispatch_part<NS>(blockIdx.y, body);
+}
+
+template <typename T, int LA, int LB, int LC, int LD>
+cudaError_t launch_jk_class(const JKParams& p, cudaStream_t s) {
+  constexpr int NS = class_split(LA, LB, LC, LD);
+  if (p.n_tasks == 0) return cudaSuccess;
+  dim3 grid((p.n_tasks + 3) / 4, NS);
+  jk_kernel<T, LA, LB, LC, LD><<<grid, 128, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+// Quartet classes evaluated by the register kernels (L <= 6); (dd|dp) and
+// (dd|dd) go to the warp-cooperative engine.
+#define JQC_FOR_REG_CLASSES(X) JQC_FOR_REG_CLASSES_LO(X) JQC_FOR_REG_CLASSES_HI(X)
+#define JQC_FOR_REG_CLASSES_LO(X) \
+  X(0, 0, 0, 0, 0)             \
+  X(1, 1, 0, 0, 0)             \
+  X(2, 1, 0, 1, 0)             \
+  X(3, 1, 1, 0, 0)             \
+  X(4, 1, 1, 1, 0)             \
+  X(5, 1, 1, 1, 1)             \
+  X(6, 2, 0, 0, 0)             \
+  X(7, 2, 0, 1, 0)             \
+  X(8, 2, 0, 1, 1)             \
+  X(9, 2, 0, 2, 0)
+#define JQC_FOR_REG_CLASSES_HI(X) \
+  X(10, 2, 1, 0, 0)            \
+  X(11, 2, 1, 1, 0)            \
+  X(12, 2, 1, 1, 1)            \
+  X(13, 2, 1, 2, 0)            \
+  X(14, 2, 1, 2, 1)            \
+  X(15, 2, 2, 0, 0)            \
+  X(16, 2, 2, 1, 0)            \
+  X(17, 2, 2, 1, 1)            \
+  X(18, 2, 2, 2, 0)
+
+// Expand a body over the 21 quartet classes (bra pair class >= ket pair class).
+#define JQC_FOR_QUARTET_CLASSES(X) \
+  X(0, 0, 0, 0, 0)                 \
+  X(1, 1, 0, 0, 0)                 \
+  X(2, 1, 0, 1, 0)                 \
+  X(3, 1, 1, 0, 0)                 \
+  X(4, 1, 1, 1, 0)                 \
+  X(5, 1, 1, 1, 1)                 \
+  X(6, 2, 0, 0, 0)                 \
+  X(7, 2, 0, 1, 0)                 \
+  X(8, 2, 0, 1, 1)                 \
+  X(9, 2, 0, 2, 0)                 \
+  X(10, 2, 1, 0, 0)                \
+  X(11, 2, 1, 1, 0)                \
+  X(12, 2, 1, 1, 1)                \
+  X(13, 2, 1, 2, 0)                \
+  X(14, 2, 1, 2, 1)                \
+  X(15, 2, 2, 0, 0)                \
+  X(16, 2, 2, 1, 0)                \
+  X(17, 2, 2, 1, 1)                \
+  X(18, 2, 2, 2, 0)                \
+  X(19, 2, 2, 2, 1)                \
+  X(20, 2, 2, 2, 2)
+
+}  // namespace jqc

@@ -1,0 +1,95 @@
+// Kernel parameter blocks and launcher declarations shared by the .cu files.
+#pragma once
+
+#include "mmd.cuh"
+
+namespace jqc {
+
+constexpr int kNumPairClasses = 6;     // (ss) (ps) (pp) (ds) (dp) (dd)
+constexpr int kNumQuartetClasses = 21; // pair class of bra >= ket
+
+__host__ __device__ constexpr int pair_class(int la, int lb) {  // la >= lb
+  return la * (la + 1) / 2 + lb;
+}
+__host__ __device__ constexpr int quartet_class(int pb, int pk) { return pb * (pb + 1) / 2 + pk; }
+
+struct JKParams {
+  const Task* tasks;
+  int n_tasks;
+  const ShellPair* pairs;
+  const void* pp;          // PrimPair* (FP64) or PrimPairF* (FP32)
+  const double* centres;   // 3 per shell
+  const int* ao;           // first basis function of each shell
+  const void* boys;        // Boys table of the kernel's type
+  const double* D;         // n_dens x n x n
+  double* J;               // n_dens x n x n (accumulated, symmetrized later)
+  double* K;
+  int n;
+  int n_dens;
+  const float* dmax;       // n_shell x n_shell max |D| per shell block, or null
+  int n_shell;
+  float dens_tau;
+};
+
+struct TensorParams {
+  const Task* tasks;
+  int n_tasks;
+  const ShellPair* pairs;
+  const PrimPair* pp;
+  const double* centres;
+  const int* ao;
+  const double* boys;
+  double* eri;
+  long long n;
+};
+
+struct SchwarzParams {
+  const int* pair_ids;     // pairs of one class
+  int n_pairs;
+  const ShellPair* pairs;
+  const PrimPair* pp;
+  const double* centres;
+  const double* boys;
+  unsigned long long* qmax;  // max (ab|ab) as ordered bits, per pair
+};
+
+struct PrimQuartetParams {
+  long long n;
+  const double* exps;      // 4 per quartet
+  const double* centres;   // 12 per quartet
+  const double* boys;
+  double* out;             // n x (nab*ncd)
+};
+
+// Launchers (return cudaError_t of the launch).
+cudaError_t launch_jk(int qc, bool fp32, const JKParams& p, cudaStream_t s);
+cudaError_t launch_eri_tensor(int qc, const TensorParams& p, cudaStream_t s);
+cudaError_t launch_schwarz(int pc, const SchwarzParams& p, cudaStream_t s);
+cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s);
+cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tab, cudaStream_t s);
+cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
+                        cudaStream_t s);
+cudaError_t launch_symmetrize(double* M, int count, int n, cudaStream_t s);
+
+// Class tables: angular momenta of pair class pc.
+__host__ __device__ constexpr int pc_la(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : 2; }
+__host__ __device__ constexpr int pc_lb(int pc) { return pc - pair_class(pc_la(pc), 0); }
+__host__ __device__ constexpr int qc_bra(int qc) {
+  int pb = 0;
+  while ((pb + 1) * (pb + 2) / 2 <= qc) ++pb;
+  return pb;
+}
+__host__ __device__ constexpr int qc_ket(int qc) { return qc - qc_bra(qc) * (qc_bra(qc) + 1) / 2; }
+__host__ __device__ constexpr int qc_L(int qc) {
+  return pc_la(qc_bra(qc)) + pc_lb(qc_bra(qc)) + pc_la(qc_ket(qc)) + pc_lb(qc_ket(qc));
+}
+// Classes with L <= 6 run in the register kernels, (dd|dp) and (dd|dd) in the
+// warp engine.
+__host__ __device__ constexpr bool is_reg_class(int qc) { return qc_L(qc) <= 6; }
+
+cudaError_t launch_warp_jk(int la, int lb, int lc, int ld, bool fp32, const JKParams& p, cudaStream_t s);
+cudaError_t launch_warp_tensor(int la, int lb, int lc, int ld, const TensorParams& p, cudaStream_t s);
+cudaError_t launch_warp_schwarz(int la, int lb, const SchwarzParams& p, cudaStream_t s);
+cudaError_t launch_warp_prim(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s);
+
+}  // namespace jqc

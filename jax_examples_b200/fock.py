@@ -1,0 +1,171 @@
+"""Fock builders (``jax_qc/scf/fock.py:31-79``) over the direct engine.
+
+``build_fock_rhf(H, D, ERI)`` and ``build_fock_uhf(H, Da, Db, ERI)`` keep the
+reference signatures; ERI may be a :class:`DirectERI` handle (fused kernels,
+no N^4 tensor) or a dense (n,n,n,n) tensor (einsum, as the reference).
+
+:class:`FockBuilder` is the stateful builder the SCF drivers use.  It adds
+the precision policy of the mixed path:
+
+* ``precision="fp64"``: every build is a full FP64 build (the plain kernel).
+* ``precision="mixed"``: quartets with Q_ij Q_kl < ``mixed_tau`` run in FP32
+  (FP64 accumulation), and with ``incremental=True`` each build contracts only
+  the density change dD = D - D_prev (J, K are linear in D) with density-
+  weighted screening, the error of which is reset by a full rebuild every
+  ``rebuild_every`` builds.  When the SCF error drops below ``fp64_switch`` the
+  builder switches to full FP64 builds, and convergence is only accepted after
+  ``fp64_tail_iters`` of them: the final energy is an FP64 energy.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+def _is_direct(ERI) -> bool:
+    return hasattr(ERI, "jk") and hasattr(ERI, "n_basis")
+
+
+def _dense_jk(D, ERI):
+    J = torch.einsum("ls,mnls->mn", D, ERI)
+    K = torch.einsum("ls,msln->mn", D, ERI)
+    return J, K
+
+
+def _as_dev(x, dev):
+    if torch.is_tensor(x):
+        return x.to(device=dev, dtype=torch.float64)
+    return torch.as_tensor(np.asarray(x), dtype=torch.float64, device=dev)
+
+
+def coulomb(D, ERI):
+    """J_mn = sum_ls D_ls (mn|ls) (``fock.py:31-33``)."""
+    if _is_direct(ERI):
+        return ERI.jk(D)[0]
+    return _dense_jk(D, ERI)[0]
+
+
+def exchange(D, ERI):
+    """K_mn = sum_ls D_ls (ms|ln) (``fock.py:36-38``)."""
+    if _is_direct(ERI):
+        return ERI.jk(D)[1]
+    return _dense_jk(D, ERI)[1]
+
+
+def build_fock_rhf(H_core, D, ERI):
+    """F = H + J - 1/2 K (``fock.py:41-47``)."""
+    if _is_direct(ERI):
+        dev = ERI.device
+        J, K = ERI.jk(_as_dev(D, dev))
+        return _as_dev(H_core, dev) + J - 0.5 * K
+    J, K = _dense_jk(D, ERI)
+    return H_core + J - 0.5 * K
+
+
+def build_fock_uhf(H_core, D_alpha, D_beta, ERI):
+    """F_s = H + J(Da+Db) - K(Ds) (``fock.py:50-79``)."""
+    if _is_direct(ERI):
+        dev = ERI.device
+        J, K = ERI.jk(torch.stack([_as_dev(D_alpha, dev), _as_dev(D_beta, dev)]))
+        H = _as_dev(H_core, dev)
+        Jt = J[0] + J[1]
+        return H + Jt - K[0], H + Jt - K[1]
+    Dt = D_alpha + D_beta
+    J = _dense_jk(Dt, ERI)[0]
+    return H_core + J - _dense_jk(D_alpha, ERI)[1], H_core + J - _dense_jk(D_beta, ERI)[1]
+
+
+class FockBuilder:
+    """Stateful J/K builder implementing the SCF precision policy."""
+
+    def __init__(self, ERI, config, rebuild_every: int = 8, dens_tau: float = 1e-12):
+        self.eri = ERI
+        self.direct = _is_direct(ERI)
+        if self.direct:
+            self.device = ERI.device
+        else:
+            self.device = ERI.device if torch.is_tensor(ERI) else torch.device("cpu")
+            if not torch.is_tensor(ERI):
+                self.eri = torch.as_tensor(np.asarray(ERI), dtype=torch.float64)
+        self.precision = getattr(config, "precision", "fp64")
+        self.mixed_tau = float(getattr(config, "mixed_tau", 1e-7))
+        self.incremental = bool(getattr(config, "incremental", False)) and self.direct
+        self.fp64_tail = int(getattr(config, "fp64_tail_iters", 2))
+        self.fp64_switch = float(getattr(config, "fp64_switch", 1e-5))
+        self.rebuild_every = rebuild_every
+        self.dens_tau = dens_tau
+        self.phase = "mixed" if (self.precision == "mixed" and self.direct) else "fp64"
+        self.fp64_builds_after_switch = 0
+        self.switched = self.phase == "fp64"
+        self._prev = None  # (D stack, J stack, K stack) of the last build
+        self._since_full = 0
+        self._events = []  # (start, end) CUDA events of every build
+        self.log = {"builds_mixed": 0, "builds_fp64": 0, "incremental_builds": 0, "jk_seconds": 0.0}
+
+    # ----------------------------------------------------------------- core
+    def _jk_stack(self, Ds):
+        D = torch.stack([_as_dev(d, self.device) for d in Ds])
+        if not self.direct:
+            J = torch.stack([_dense_jk(d, self.eri)[0] for d in D])
+            K = torch.stack([_dense_jk(d, self.eri)[1] for d in D])
+            self.log["builds_fp64"] += 1
+            return J, K
+        prec = self.phase
+        key = "builds_mixed" if prec == "mixed" else "builds_fp64"
+        self.log[key] += 1
+        if prec == "fp64":
+            self.fp64_builds_after_switch += 1 if self.switched else 0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        use_inc = self.incremental and self._prev is not None and self._since_full < self.rebuild_every
+        if use_inc and self._prev[0].shape == D.shape:
+            dD = D - self._prev[0]
+            dJ, dK = self.eri.jk(dD, precision=prec, mixed_tau=self.mixed_tau, dens_tau=self.dens_tau)
+            J = self._prev[1] + dJ
+            K = self._prev[2] + dK
+            self._since_full += 1
+            self.log["incremental_builds"] += 1
+        else:
+            J, K = self.eri.jk(D, precision=prec, mixed_tau=self.mixed_tau)
+            self._since_full = 0
+        if self.incremental:
+            self._prev = (D, J, K)
+        e1.record()
+        self._events.append((e0, e1))
+        return J, K
+
+    def jk(self, D):
+        J, K = self._jk_stack([D])
+        return J[0], K[0]
+
+    def rhf(self, H, D):
+        J, K = self._jk_stack([D])
+        return H + J[0] - 0.5 * K[0]
+
+    def uhf(self, H, Da, Db):
+        J, K = self._jk_stack([Da, Db])
+        Jt = J[0] + J[1]
+        return H + Jt - K[0], H + Jt - K[1]
+
+    # --------------------------------------------------------------- policy
+    def observe(self, err_max: float) -> None:
+        """Called once per SCF iteration with max|DIIS error|."""
+        if self.phase == "mixed" and err_max < self.fp64_switch:
+            self.phase = "fp64"
+            self.switched = True
+            self._prev = None  # next build is a full FP64 build
+
+    def converged_ok(self) -> bool:
+        if self.precision != "mixed" or not self.direct:
+            return True
+        return self.phase == "fp64" and self.fp64_builds_after_switch >= self.fp64_tail
+
+    def record(self) -> dict:
+        """Build counters and the device time of all J/K builds (CUDA events)."""
+        if self._events:
+            self._events[-1][1].synchronize()
+            self.log["jk_seconds"] = sum(a.elapsed_time(b) for a, b in self._events) * 1e-3
+        return dict(self.log, precision=self.precision, mixed_tau=self.mixed_tau,
+                    incremental=self.incremental)
