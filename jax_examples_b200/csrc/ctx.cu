@@ -221,7 +221,7 @@ static void make_prim_pairs(const jqc_ctx* c, int a, int b, std::vector<PrimPair
       q.K = std::exp(-(al * be / p) * ab2) * c->coefs[c->prim_off[a] + i] * c->coefs[c->prim_off[b] + j];
       q.alpha = al;
       q.beta = be;
-      q.pad = 0.0;
+      q.h = 0.5 / p;
       out.push_back(q);
     }
 }
@@ -571,7 +571,7 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
       const PrimPair& q = rawpp[src + k];
       pp.push_back(q);
       ppf.push_back(PrimPairF{float(q.p), float(q.Px), float(q.Py), float(q.Pz), float(q.K), float(q.alpha),
-                              float(q.beta), 0.f});
+                              float(q.beta), float(q.h)});
     }
     auto kk = key(keep[r]);
     if (c->blocks.empty() || std::get<0>(kk) != c->blocks.back().pc || std::get<1>(kk) != c->blocks.back().ka ||

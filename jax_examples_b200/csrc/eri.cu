@@ -88,13 +88,13 @@ struct PrimBody {
       const double al = ex[0], be = ex[1], p = al + be;
       const double dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
       bra = PrimPair{p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
-                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.0};
+                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
     }
     {
       const double al = ex[2], be = ex[3], p = al + be;
       const double dx = C.x - D.x, dy = C.y - D.y, dz = C.z - D.z;
       ket = PrimPair{p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
-                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.0};
+                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
     }
     double out[Cfg::NAB][Cfg::CDP];
     double ebuf[3][LA + 1][LB + 1][LA + LB + 1];

@@ -18,12 +18,13 @@
 namespace jqc {
 
 // One primitive pair of a shell pair (a, b): p = alpha + beta,
-// P = (alpha A + beta B) / p, K = exp(-alpha beta |AB|^2 / p) c_a c_b.
+// P = (alpha A + beta B) / p, K = exp(-alpha beta |AB|^2 / p) c_a c_b,
+// h = 1/(2p) (kept so no kernel divides by p).
 struct __align__(16) PrimPair {
-  double p, Px, Py, Pz, K, alpha, beta, pad;
+  double p, Px, Py, Pz, K, alpha, beta, h;
 };
 struct __align__(16) PrimPairF {
-  float p, Px, Py, Pz, K, alpha, beta, pad;
+  float p, Px, Py, Pz, K, alpha, beta, h;
 };
 template <typename T>
 struct PPType;
@@ -162,15 +163,15 @@ __device__ __forceinline__ float fast_rsqrt(float x) { return rsqrtf(x); }
 template <typename T, int L, typename PPT>
 __device__ __forceinline__ void prim_quartet_R(const PPT& bp, const PPT& kp, const T* __restrict__ boys_tab,
                                                T (&R)[nherm(L)]) {
+  // 1/(p+q) = r^2 with r = 1/sqrt(p+q); 1/(pq) = 4 h_p h_q: no divisions.
   const T p = bp.p, q = kp.p;
-  const T pq = p * q;
-  const T ipq = T(1) / (p + q);
-  const T rho = pq * ipq;
+  const T r = fast_rsqrt(p + q);
+  const T rho = p * q * (r * r);
   const T PQx = bp.Px - kp.Px, PQy = bp.Py - kp.Py, PQz = bp.Pz - kp.Pz;
   const T tb = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
   T F[L + 1];
   boys_eval<T, L>(tb, boys_tab, F);
-  T pref = T(kTwoPi25) * T(bp.K) * T(kp.K) * fast_rsqrt(p + q) / pq;
+  T pref = T(4.0 * kTwoPi25) * T(bp.K) * T(kp.K) * (T(bp.h) * T(kp.h)) * r;
   T Rn[L + 1];
   const T m2rho = T(-2) * rho;
   static_for<L + 1>([&](auto nn) {
@@ -203,7 +204,7 @@ __device__ __forceinline__ void quartet_accumulate(
     const int lane = threadIdx.x & 31;
     for (int ip = 0; ip < nbra; ++ip) {
       const auto bp = bra[ip];
-      const T inv2p = T(0.5) / T(bp.p);
+      const T inv2p = bp.h;
       if constexpr (SHARED_BRA) {
         __syncwarp();
         if (lane == 0) ecoef_compute<T, LA, LB, false>(ebra[0], bp.Px - A.x, bp.Px - B.x, inv2p);
@@ -218,7 +219,7 @@ __device__ __forceinline__ void quartet_accumulate(
       const EArr<T, LA, LB> Ex = ebra[0], Ey = ebra[1], Ez = ebra[2];
       for (int iq = 0; iq < nket; ++iq) {
         const auto kp = ket[iq];
-        const T inv2q = T(0.5) / T(kp.p);
+        const T inv2q = kp.h;
         T fbuf[3][LC + 1][LD + 1][LC + LD + 1];
         ecoef_compute<T, LC, LD, true>(fbuf[0], kp.Px - C.x, kp.Px - D.x, inv2q);
         ecoef_compute<T, LC, LD, true>(fbuf[1], kp.Py - C.y, kp.Py - D.y, inv2q);

@@ -143,27 +143,27 @@ struct WarpQuartet {
   }
 
   // Bra E for one bra primitive pair (all lanes call).
-  __device__ __forceinline__ void set_bra(T Px, T Py, T Pz, T p, Vec3<T> A, Vec3<T> B) {
+  __device__ __forceinline__ void set_bra(T Px, T Py, T Pz, T hp, Vec3<T> A, Vec3<T> B) {
     __syncwarp();
-    const T inv2p = T(0.5) / p;
+    const T inv2p = hp;
     if (lane == 0) wecoef<T>(sm->E[0][0], la, lb, Px - A.x, Px - B.x, inv2p, false);
     if (lane == 1) wecoef<T>(sm->E[0][1], la, lb, Py - A.y, Py - B.y, inv2p, false);
     if (lane == 2) wecoef<T>(sm->E[0][2], la, lb, Pz - A.z, Pz - B.z, inv2p, false);
   }
 
   // One primitive quartet (all lanes call with the same arguments).
-  __device__ __forceinline__ void add_prim(T p, T Px, T Py, T Pz, T Kab, T q, T Qx, T Qy, T Qz, T Kcd, Vec3<T> C,
-                                           Vec3<T> D, const T* __restrict__ tab) {
-    const T inv2q = T(0.5) / q;
+  __device__ __forceinline__ void add_prim(T p, T hp, T Px, T Py, T Pz, T Kab, T q, T hq, T Qx, T Qy, T Qz, T Kcd,
+                                           Vec3<T> C, Vec3<T> D, const T* __restrict__ tab) {
+    const T inv2q = hq;
     if (lane == 3) wecoef<T>(sm->E[1][0], lc, ld, Qx - C.x, Qx - D.x, inv2q, true);
     if (lane == 4) wecoef<T>(sm->E[1][1], lc, ld, Qy - C.y, Qy - D.y, inv2q, true);
     if (lane == 5) wecoef<T>(sm->E[1][2], lc, ld, Qz - C.z, Qz - D.z, inv2q, true);
-    const T pq = p * q;
-    const T rho = pq / (p + q);
+    const T r = fast_rsqrt(p + q);
+    const T rho = p * q * (r * r);
     const T X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;
     const T tb = rho * (X * X + Y * Y + Z * Z);
     if (lane <= L) {
-      T pref = T(kTwoPi25) * Kab * Kcd * fast_rsqrt(p + q) / pq;
+      T pref = T(4.0 * kTwoPi25) * Kab * Kcd * (hp * hq) * r;
       const T m2rho = T(-2) * rho;
       for (int k = 0; k < lane; ++k) pref *= m2rho;
       sm->Rn[lane] = pref * boys_single<T>(tb, lane, tab);

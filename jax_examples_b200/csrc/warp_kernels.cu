@@ -17,11 +17,11 @@ __device__ __forceinline__ void warp_contract_pair(WarpQuartet<T>& wq, const typ
                                                    int nket, Vec3<T> C, Vec3<T> D, const T* tab) {
   for (int ip = 0; ip < nbra; ++ip) {
     const auto bp = bra[ip];
-    wq.set_bra(T(bp.Px), T(bp.Py), T(bp.Pz), T(bp.p), A, B);
+    wq.set_bra(T(bp.Px), T(bp.Py), T(bp.Pz), T(bp.h), A, B);
     for (int iq = 0; iq < nket; ++iq) {
       const auto kp = ket[iq];
-      wq.add_prim(T(bp.p), T(bp.Px), T(bp.Py), T(bp.Pz), T(bp.K), T(kp.p), T(kp.Px), T(kp.Py), T(kp.Pz), T(kp.K), C,
-                  D, tab);
+      wq.add_prim(T(bp.p), T(bp.h), T(bp.Px), T(bp.Py), T(bp.Pz), T(bp.K), T(kp.p), T(kp.h), T(kp.Px), T(kp.Py),
+                  T(kp.Pz), T(kp.K), C, D, tab);
     }
   }
   wq.publish();
@@ -203,13 +203,13 @@ __global__ void __launch_bounds__(kWarpBlock) warp_prim_kernel(const PrimQuartet
     const double al = ex[0], be = ex[1], p = al + be;
     const double dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
     bra = PrimPair{p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
-                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.0};
+                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
   }
   {
     const double al = ex[2], be = ex[3], p = al + be;
     const double dx = C.x - D.x, dy = C.y - D.y, dz = C.z - D.z;
     ket = PrimPair{p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
-                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.0};
+                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
   }
   WarpQuartet<double> wq;
   wq.sm = sm;
