@@ -114,6 +114,22 @@ int jqc_one_electron(jqc_ctx *ctx, double *S, double *T, double *V, void *stream
 int jqc_jk(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode, double mixed_tau,
            double dens_tau, void *stream);
 
+/* Allocation-free variant of jqc_jk for callers that cannot allocate device
+ * memory when they need a Fock build: a builder called from inside a JAX/XLA
+ * program (XLA owns and pre-reserves device memory) or a fixed-memory host
+ * loop.  No reference counterpart.  Same arguments and results as jqc_jk with
+ * density screening at dens_tau (0 disables it).  Allocates nothing: the
+ * work list must already exist (call jqc_jk or jqc_stats once with the same
+ * precision_mode/mixed_tau at set-up; otherwise JQC_ERR_NOT_READY), and the
+ * density-screening scratch is a static device array of 512*512 floats, so
+ * contexts with more than 512 shells get JQC_ERR_TOO_LARGE.  The first call
+ * on a device looks the array's address up (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the array and each
+ * call rewrites it completely before reading it; calls that overlap on the
+ * GPU (different streams or contexts without ordering) race on it. */
+int jqc_jk_noalloc(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode,
+                   double mixed_tau, double dens_tau, void *stream);
+
 /* jqc_jk with the class kernels run one after another on `stream`, each
  * timed with CUDA events; class_ms[p*21+q] receives milliseconds (0 for
  * empty classes).  Synchronizes.  Measurement variant of jqc_jk. */

@@ -839,3 +839,72 @@ static int jk_impl(jqc_ctx* c, int n_dens, const double* D, double* J, double* K
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Support for the allocation-free entry point (noalloc.cu).  Runs the J/K
+// build of a context whose work list for (precision_mode, mixed_tau) already
+// exists, with the per-shell-pair density maxima written to `dmax_scratch`
+// (capacity in floats) supplied by the caller.  Never builds a work list and
+// never allocates device memory.
+namespace jqc {
+
+int ctx_device(const jqc_ctx* c) { return c ? c->device : -1; }
+
+int jk_run_preallocated(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, int precision_mode,
+                        double mixed_tau, double dens_tau, float* dmax_scratch, size_t dmax_capacity,
+                        cudaStream_t s) {
+  JQC_REQUIRE(c && D && J && K && dmax_scratch, JQC_ERR_INVALID, "jqc_jk_noalloc: null argument");
+  JQC_REQUIRE(n_dens >= 1 && n_dens <= 4, JQC_ERR_INVALID, "jqc_jk_noalloc: n_dens must be 1..4");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_jk_noalloc: call jqc_pairs_build first");
+  JQC_REQUIRE(precision_mode >= 0 && precision_mode <= 2, JQC_ERR_INVALID, "jqc_jk_noalloc: bad precision_mode");
+  JQC_REQUIRE(mixed_tau >= 0.0 && dens_tau >= 0.0, JQC_ERR_INVALID, "jqc_jk_noalloc: thresholds must be >= 0");
+  JQC_REQUIRE((size_t)c->n_shell * c->n_shell <= dmax_capacity, JQC_ERR_TOO_LARGE,
+              "jqc_jk_noalloc: n_shell^2 exceeds the static scratch (at most 512 shells)");
+  const double key_tau = precision_mode == JQC_PREC_MIXED ? mixed_tau : 0.0;
+  TaskSet* ts = nullptr;
+  for (TaskSet* t : c->jk_cache)
+    if (t->valid && t->mode == precision_mode && t->mixed_tau == key_tau) ts = t;
+  JQC_REQUIRE(ts != nullptr, JQC_ERR_NOT_READY,
+              "jqc_jk_noalloc: no work list for this precision_mode/mixed_tau; call jqc_jk (or jqc_stats) once "
+              "with the same settings first, at a point where allocation is allowed");
+  int rc = select_device(c);
+  if (rc) return rc;
+  const int n = c->n_bf;
+  const size_t nn = (size_t)n * n * n_dens;
+  JQC_CUDA_CHECK(cudaMemsetAsync(J, 0, nn * sizeof(double), s));
+  JQC_CUDA_CHECK(cudaMemsetAsync(K, 0, nn * sizeof(double), s));
+  JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, dmax_scratch, s));
+  JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
+  for (int i = 0; i < kNumStreams; ++i) JQC_CUDA_CHECK(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
+  int li = 0;
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      JKParams p;
+      p.tasks = ts->d.ptr + ts->off[prec][qc];
+      p.n_tasks = ts->cnt[prec][qc];
+      if (p.n_tasks == 0) continue;
+      p.pairs = c->d_pairs.ptr;
+      p.pp = prec ? (const void*)c->d_ppf.ptr : (const void*)c->d_pp.ptr;
+      p.centres = c->d_centres.ptr;
+      p.ao = c->d_ao.ptr;
+      p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
+      p.D = D;
+      p.J = J;
+      p.K = K;
+      p.n = n;
+      p.n_dens = n_dens;
+      p.dmax = dmax_scratch;
+      p.n_shell = c->n_shell;
+      p.dens_tau = (float)dens_tau;
+      JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, c->side[li++ % kNumStreams]));
+    }
+  for (int i = 0; i < kNumStreams; ++i) {
+    JQC_CUDA_CHECK(cudaEventRecord(c->ev_join[i], c->side[i]));
+    JQC_CUDA_CHECK(cudaStreamWaitEvent(s, c->ev_join[i], 0));
+  }
+  JQC_CUDA_CHECK(launch_symmetrize(J, n_dens, n, s));
+  JQC_CUDA_CHECK(launch_symmetrize(K, n_dens, n, s));
+  return JQC_OK;
+}
+
+}  // namespace jqc
