@@ -105,6 +105,23 @@ int jqc_eri_tensor(jqc_ctx *ctx, double *out_n4, long long max_bytes, void *stre
  * nuclear.py:62-81 (compute_overlap/kinetic/nuclear_matrix). */
 int jqc_one_electron(jqc_ctx *ctx, double *S, double *T, double *V, void *stream);
 
+/* Two-electron part of the nuclear gradient, ADDED into grad (n_atom x 3,
+ * device, caller zeroes): grad += 1/2 sum Gamma_abcd d(ab|cd)/dR with
+ * Gamma = j_scale D^t_ab D^t_cd - (k_scale/2) sum_s (D^s_ac D^s_bd +
+ * D^s_ad D^s_bc), D^t = sum_s D^s over the n_dens densities.  RHF: one total
+ * density, j_scale = 1, k_scale = 1/2; UHF: (D_alpha, D_beta), 1, 1.  The
+ * derivative integrals are contracted on the fly and never stored.
+ * Replaces the finite-difference ERI derivative and its contraction in
+ * grad/rhf_grad.py:153-209 (dERI, dJ, dK). */
+int jqc_grad2e(jqc_ctx *ctx, int n_dens, const double *D, double j_scale, double k_scale, double *grad,
+               void *stream);
+
+/* One-electron part of the nuclear gradient, ADDED into grad:
+ * grad += sum D_ab d(T+V)_ab/dR - sum W_ab dS_ab/dR (Hellmann-Feynman term of
+ * V included); D total density, W energy-weighted density (n x n, device).
+ * Replaces the dH/dS finite differences of grad/rhf_grad.py:186-209. */
+int jqc_grad1e(jqc_ctx *ctx, const double *D, const double *W, double *grad, void *stream);
+
 /* Direct J/K (the N^4 tensor is never stored): for each of n_dens densities
  * D[d] (n x n, symmetric), J[d] = sum_ls D_ls (mn|ls), K[d] = sum_ls D_ls
  * (ms|ln).  precision_mode as JQC_PREC_*, mixed_tau the FP32/FP64 split on

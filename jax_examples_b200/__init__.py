@@ -17,13 +17,14 @@ from .core import (
 )
 from .engine import DirectERI, boys, eri_prim_quartets
 from .fock import build_fock_rhf, build_fock_uhf
+from .grad import compute_gradient, numerical_gradient, rhf_gradient, uhf_gradient
 from .integrals import compute_eri_tensor, compute_integrals, nuclear_repulsion_energy
 from .profiling import StageTimer
 from .scf import run_rhf, run_scf, run_uhf
 
 __all__ = [
     "BasisSet", "CalcConfig", "DirectERI", "IntegralSet", "Molecule", "SCFResult", "SCFState", "Shell",
-    "StageTimer", "boys", "build_basis_set", "build_fock_rhf", "build_fock_uhf", "compute_eri_tensor",
+    "StageTimer", "boys", "compute_gradient", "numerical_gradient", "rhf_gradient", "uhf_gradient", "build_basis_set", "build_fock_rhf", "build_fock_uhf", "compute_eri_tensor",
     "compute_integrals", "eri_prim_quartets", "make_molecule", "nuclear_repulsion_energy", "register_basis",
     "run_rhf", "run_scf", "run_uhf", "water_cluster", "water_monomer_bohr",
 ]

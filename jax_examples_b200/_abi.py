@@ -63,6 +63,8 @@ SIGNATURES = {
     "jqc_eri_tensor": (_c_int, [_vp, _vp, _c_ll, _vp]),
     "jqc_one_electron": (_c_int, [_vp, _vp, _vp, _vp, _vp]),
     "jqc_jk": (_c_int, [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_dbl, _c_dbl, _vp]),
+    "jqc_grad2e": (_c_int, [_vp, _c_int, _vp, _c_dbl, _c_dbl, _vp, _vp]),
+    "jqc_grad1e": (_c_int, [_vp, _vp, _vp, _vp, _vp]),
     "jqc_jk_noalloc": (_c_int, [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_dbl, _c_dbl, _vp]),
     "jqc_jk_timed": (_c_int, [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_dbl, _c_dbl, _vp, _dp]),
     "jqc_class_stats": (_c_int, [_vp, _c_int, _c_dbl, _llp]),

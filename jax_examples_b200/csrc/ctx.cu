@@ -194,6 +194,7 @@ struct jqc_ctx {
   std::vector<TaskSet*> jk_cache;
   TaskSet* jk_cur = nullptr;
   TaskSet full_tasks;
+  TaskSet grad_tasks;  // one screened quartet per task, whole contractions
   // scratch
   DevBuf<float> d_dmax;
   cudaStream_t side[kNumStreams] = {};
@@ -241,7 +242,8 @@ static int prefix_count(const std::vector<ShellPair>& pairs, int start, int limi
   return lo;
 }
 
-static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s) {
+static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s,
+                       bool grad = false) {
   std::vector<Task> lists[2][kNumQuartetClasses];
   long long nq[2] = {0, 0}, npq = 0;
   long long cq[2][kNumQuartetClasses] = {}, cp[2][kNumQuartetClasses] = {};
@@ -264,10 +266,10 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
         // primitive quartets per task (the tensor keeps whole quartets).
         const int nbp = c->pairs[gi].npp, nkp = K.ka * K.kb;
         int chunk = nbp;
-        if (!full) chunk = std::max(1, std::min(nbp, kMaxLanePrims / std::max(1, nkp)));
+        if (!full && !grad) chunk = std::max(1, std::min(nbp, kMaxLanePrims / std::max(1, nkp)));
         // Register classes: 32 kets per warp task (one per lane).  Warp-engine
         // classes: one ket per task, so every quartet gets its own warp.
-        const int per_task = is_reg_class(qc) ? 32 : 1;
+        const int per_task = (is_reg_class(qc) && !grad) ? 32 : 1;
         for (int prec = 0; prec < 2; ++prec) {
           for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
             for (int b0 = 0; b0 < nbp; b0 += chunk) {
@@ -473,6 +475,7 @@ int jqc_basis_upload(jqc_ctx* c, int n_shell, const int* l, const int* nprim, co
   c->pairs_ready = false;
   drop_jk_tasks(c);
   c->full_tasks.valid = false;
+  c->grad_tasks.valid = false;
   return JQC_OK;
 }
 
@@ -589,6 +592,7 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
   c->pairs_ready = true;
   drop_jk_tasks(c);
   c->full_tasks.valid = false;
+  c->grad_tasks.valid = false;
   return JQC_OK;
 }
 
@@ -720,6 +724,70 @@ int jqc_eri_tensor(jqc_ctx* c, double* out, long long max_bytes, void* stream) {
     p.n = c->n_bf;
     JQC_CUDA_CHECK(launch_eri_tensor(qc, p, s));
   }
+  return JQC_OK;
+}
+
+int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k_scale, double* grad,
+               void* stream) {
+  JQC_REQUIRE(c && D && grad, JQC_ERR_INVALID, "jqc_grad2e: null argument");
+  JQC_REQUIRE(n_dens >= 1 && n_dens <= 4, JQC_ERR_INVALID, "jqc_grad2e: n_dens must be 1..4");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_grad2e: call jqc_pairs_build first");
+  JQC_REQUIRE(c->n_atom > 0, JQC_ERR_NOT_READY, "jqc_grad2e: the basis was uploaded without atoms");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!c->grad_tasks.valid) {
+    rc = build_tasks(c, c->grad_tasks, JQC_PREC_FP64, 0.0, false, s, true);
+    if (rc) return rc;
+  }
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    GradParams p;
+    p.tasks = c->grad_tasks.d.ptr + c->grad_tasks.off[0][qc];
+    p.n_tasks = c->grad_tasks.cnt[0][qc];
+    if (p.n_tasks == 0) continue;
+    p.pairs = c->d_pairs.ptr;
+    p.pp = c->d_pp.ptr;
+    p.centres = c->d_centres.ptr;
+    p.ao = c->d_ao.ptr;
+    p.atom = c->d_atom.ptr;
+    p.boys = c->boys64;
+    p.D = D;
+    p.n_dens = n_dens;
+    p.n = c->n_bf;
+    p.jscale = j_scale;
+    p.kscale = k_scale;
+    p.grad = grad;
+    const int pb = qc_bra(qc), pk = qc_ket(qc);
+    JQC_CUDA_CHECK(launch_warp_grad(pc_la(pb), pc_lb(pb), pc_la(pk), pc_lb(pk), p, s));
+  }
+  return JQC_OK;
+}
+
+int jqc_grad1e(jqc_ctx* c, const double* D, const double* W, double* grad, void* stream) {
+  JQC_REQUIRE(c && D && W && grad, JQC_ERR_INVALID, "jqc_grad1e: null argument");
+  JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_grad1e: call jqc_basis_upload first");
+  JQC_REQUIRE(c->n_atom > 0, JQC_ERR_NOT_READY, "jqc_grad1e: the basis was uploaded without atoms");
+  int rc = select_device(c);
+  if (rc) return rc;
+  Grad1Params p;
+  p.n_shell = c->n_shell;
+  p.n = c->n_bf;
+  p.n_atom = c->n_atom;
+  p.l = c->d_l.ptr;
+  p.nprim = c->d_nprim.ptr;
+  p.prim_off = c->d_prim_off.ptr;
+  p.exps = c->d_exps.ptr;
+  p.coefs = c->d_coefs.ptr;
+  p.centres = c->d_centres.ptr;
+  p.ao = c->d_ao.ptr;
+  p.atom = c->d_atom.ptr;
+  p.atom_xyz = c->d_atom_xyz.ptr;
+  p.atom_Z = c->d_atom_Z.ptr;
+  p.boys = c->boys64;
+  p.D = D;
+  p.W = W;
+  p.grad = grad;
+  JQC_CUDA_CHECK(launch_grad1e(p, static_cast<cudaStream_t>(stream)));
   return JQC_OK;
 }
 

@@ -1,0 +1,503 @@
+// Nuclear-gradient kernels: the ERI-derivative adjoint and the one-electron
+// derivative terms.
+//
+// Two-electron part.  With Gamma_abcd = j D^t_ab D^t_cd
+//     - (k/2) sum_s (D^s_ac D^s_bd + D^s_ad D^s_bc)   (D^t = sum_s D^s)
+// the two-electron energy is E2 = 1/2 sum Gamma (ab|cd) and its nuclear
+// gradient 1/2 sum Gamma d(ab|cd)/dR.  RHF: one density, j = 1, k = 1/2,
+// which is the contraction rhf_grad.py:201-209 forms from finite differences
+// (1/2 sum D (dJ - dK/2)); UHF: alpha and beta densities, j = k = 1.  Over
+// canonical shell quartets that is 4 s sum_elements Gamma d(ab|cd)/dR with the
+// usual 1/2 per coincidence in s.
+//
+// The derivative integrals are never stored.  Per primitive quartet:
+//   d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}
+// enters as derivative E coefficients DA^x_{ij,t} = 2 alpha E_{i+1,j,t} -
+// i E_{i-1,j,t} (likewise DB with beta on the bra's second centre and DC with
+// gamma on the ket's first centre), contracted with the same R_tuv and the
+// ket/bra E coefficients as the integrals themselves; dD follows from
+// translational invariance, dD = -(dA + dB + dC).  The bra derivatives use
+// X_cd[tuv] (ket contracted against R) up to one higher bra Hermite order,
+// the ket derivative a second pass of stage 1 with DC.
+//
+// This file holds the warp-cooperative version (runtime class, one warp per
+// shell quartet, R/E/X/Gamma in shared memory); it serves every class.
+#include "kernels.cuh"
+#include "warp_engine.cuh"
+
+namespace jqc {
+
+constexpr int kGMaxL = 9;                       // (dd|dd) + 1
+constexpr int kGMaxHerm = nherm(kGMaxL);        // 220
+constexpr int kGMaxX = 36 * nherm(5);           // ncd * nherm(LAB+1) <= 36 * 56
+
+struct GradSmem {
+  double R[kGMaxHerm];
+  double Rn[kGMaxL + 2];
+  double Eb[3][4][4][7];   // bra E, i <= la+1, j <= lb+1, t <= la+lb+2
+  double DA[3][3][3][6];   // derivative E on centre A, i <= la, j <= lb, t <= la+lb+1
+  double DB[3][3][3][6];
+  double Fk[3][4][3][6];   // ket E with (-1)^t, c <= lc+1, d <= ld
+  double DC[3][3][3][6];   // derivative ket E on centre C (signed)
+  double X[kGMaxX];
+  double G[36 * 36];       // Gamma_abcd
+};
+
+// E coefficients (runtime la, lb) along one axis into e[i][j][t] for
+// i <= la, j <= lb, with capacity [4][4][7].
+__device__ void gecoef(double (*e)[4][7], int la, int lb, double pa, double pb, double inv2p) {
+  for (int i = 0; i <= la; ++i)
+    for (int j = 0; j <= lb; ++j)
+      for (int t = 0; t < 7; ++t) e[i][j][t] = 0.0;
+  e[0][0][0] = 1.0;
+  for (int i = 0; i < la; ++i)
+    for (int t = 0; t <= i + 1; ++t) {
+      double v = 0.0;
+      if (t <= i) v = pa * e[i][0][t];
+      if (t >= 1) v += inv2p * e[i][0][t - 1];
+      if (t + 1 <= i) v += (t + 1) * e[i][0][t + 1];
+      e[i + 1][0][t] = v;
+    }
+  for (int j = 0; j < lb; ++j)
+    for (int i = 0; i <= la; ++i)
+      for (int t = 0; t <= i + j + 1; ++t) {
+        double v = 0.0;
+        if (t <= i + j) v = pb * e[i][j][t];
+        if (t >= 1) v += inv2p * e[i][j][t - 1];
+        if (t + 1 <= i + j) v += (t + 1) * e[i][j][t + 1];
+        e[i][j + 1][t] = v;
+      }
+}
+
+__global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int la, int lb, int lc, int ld) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  GradSmem* sm = reinterpret_cast<GradSmem*>(smraw);
+  const int lane = threadIdx.x & 31;
+  const int task_id = blockIdx.x;
+  if (task_id >= prm.n_tasks) return;
+  const Task task = prm.tasks[task_id];
+  const ShellPair bp = prm.pairs[task.bra];
+  const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
+  const int nab = na * nb, ncd = nc * nd, ntot = nab * ncd;
+  const int lab = la + lb, L = la + lb + lc + ld;
+  const int nh1 = nherm(lab + 1), nh0 = nherm(lab);
+  const int n = prm.n;
+  const double* ctr = prm.centres;
+  const double Ax = ctr[3 * bp.a], Ay = ctr[3 * bp.a + 1], Az = ctr[3 * bp.a + 2];
+  const double Bx = ctr[3 * bp.b], By = ctr[3 * bp.b + 1], Bz = ctr[3 * bp.b + 2];
+  const int a0 = prm.ao[bp.a], b0 = prm.ao[bp.b];
+
+  for (int kk = 0; kk < task.nket; ++kk) {
+    const int kidx = task.ket0 + kk;
+    const ShellPair kp = prm.pairs[kidx];
+    const double Cx = ctr[3 * kp.a], Cy = ctr[3 * kp.a + 1], Cz = ctr[3 * kp.a + 2];
+    const double Dx = ctr[3 * kp.b], Dy = ctr[3 * kp.b + 1], Dz = ctr[3 * kp.b + 2];
+    const int c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];
+    // Gamma for this quartet
+    __syncwarp();
+    for (int e = lane; e < ntot; e += 32) {
+      const int ab = e / ncd, cd = e % ncd;
+      const int ia = a0 + ab / nb, ib = b0 + ab % nb, ic = c0 + cd / nd, id = d0 + cd % nd;
+      double dab = 0.0, dcd = 0.0, kx = 0.0;
+      for (int s = 0; s < prm.n_dens; ++s) {
+        const double* Ds = prm.D + (size_t)s * n * n;
+        dab += Ds[(size_t)ia * n + ib];
+        dcd += Ds[(size_t)ic * n + id];
+        kx += Ds[(size_t)ia * n + ic] * Ds[(size_t)ib * n + id] + Ds[(size_t)ia * n + id] * Ds[(size_t)ib * n + ic];
+      }
+      sm->G[e] = prm.jscale * dab * dcd - 0.5 * prm.kscale * kx;
+    }
+    double g[9];
+    for (int k = 0; k < 9; ++k) g[k] = 0.0;
+
+    for (int ip = 0; ip < bp.npp; ++ip) {
+      const PrimPair bpp = prm.pp[bp.pp + ip];
+      __syncwarp();
+      if (lane < 3) {
+        const double P = lane == 0 ? bpp.Px : lane == 1 ? bpp.Py : bpp.Pz;
+        const double A = lane == 0 ? Ax : lane == 1 ? Ay : Az;
+        const double B = lane == 0 ? Bx : lane == 1 ? By : Bz;
+        double(*E)[4][7] = sm->Eb[lane];
+        gecoef(E, la + 1, lb + 1, P - A, P - B, bpp.h);
+        for (int i = 0; i <= la; ++i)
+          for (int j = 0; j <= lb; ++j)
+            for (int t = 0; t <= la + lb + 1; ++t) {
+              double va = 2.0 * bpp.alpha * E[i + 1][j][t];
+              if (i > 0) va -= i * E[i - 1][j][t];
+              double vb = 2.0 * bpp.beta * E[i][j + 1][t];
+              if (j > 0) vb -= j * E[i][j - 1][t];
+              sm->DA[lane][i][j][t] = va;
+              sm->DB[lane][i][j][t] = vb;
+            }
+      }
+      for (int iq = 0; iq < kp.npp; ++iq) {
+        const PrimPair kpp = prm.pp[kp.pp + iq];
+        if (lane >= 3 && lane < 6) {
+          const int ax = lane - 3;
+          const double Q = ax == 0 ? kpp.Px : ax == 1 ? kpp.Py : kpp.Pz;
+          const double C = ax == 0 ? Cx : ax == 1 ? Cy : Cz;
+          const double Dd = ax == 0 ? Dx : ax == 1 ? Dy : Dz;
+          double(*F)[3][6] = sm->Fk[ax];
+          double tmp[4][4][7];
+          gecoef(tmp, lc + 1, ld, Q - C, Q - Dd, kpp.h);
+          for (int c = 0; c <= lc + 1; ++c)
+            for (int d = 0; d <= ld; ++d)
+              for (int t = 0; t < 6; ++t) F[c][d][t] = (t & 1) ? -tmp[c][d][t] : tmp[c][d][t];
+          for (int c = 0; c <= lc; ++c)
+            for (int d = 0; d <= ld; ++d)
+              for (int t = 0; t < 6; ++t) {
+                double v = 2.0 * kpp.alpha * F[c + 1][d][t];
+                if (c > 0) v -= c * F[c - 1][d][t];
+                sm->DC[ax][c][d][t] = v;
+              }
+        }
+        // Boys and R up to L+1
+        const double r = rsqrt(bpp.p + kpp.p);
+        const double rho = bpp.p * kpp.p * (r * r);
+        const double X = bpp.Px - kpp.Px, Y = bpp.Py - kpp.Py, Z = bpp.Pz - kpp.Pz;
+        const double tb = rho * (X * X + Y * Y + Z * Z);
+        const int L1 = L + 1;
+        if (lane <= L1) {
+          double pref = 4.0 * kTwoPi25 * bpp.K * kpp.K * (bpp.h * kpp.h) * r;
+          for (int k = 0; k < lane; ++k) pref *= -2.0 * rho;
+          sm->Rn[lane] = pref * boys_single<double>(tb, lane, prm.boys);
+        }
+        __syncwarp();
+        if (lane == 0) sm->R[0] = sm->Rn[L1];
+        __syncwarp();
+        for (int m = L1 - 1; m >= 0; --m) {
+          for (int s = L1 - m; s >= 1; --s) {
+            const int base = s * (s + 1) * (s + 2) / 6;
+            for (int k = lane; k < ncart(s); k += 32) {
+              int t, u, v;
+              wcart(s, k, t, u, v);
+              double val;
+              if (t > 0) {
+                val = X * sm->R[herm_index(t - 1, u, v)];
+                if (t > 1) val += (t - 1) * sm->R[herm_index(t - 2, u, v)];
+              } else if (u > 0) {
+                val = Y * sm->R[herm_index(t, u - 1, v)];
+                if (u > 1) val += (u - 1) * sm->R[herm_index(t, u - 2, v)];
+              } else {
+                val = Z * sm->R[herm_index(t, u, v - 1)];
+                if (v > 1) val += (v - 1) * sm->R[herm_index(t, u, v - 2)];
+              }
+              sm->R[base + k] = val;
+            }
+            __syncwarp();
+          }
+          if (lane == 0) sm->R[0] = sm->Rn[m];
+          __syncwarp();
+        }
+        // stage 1: X[cd][h], h < nherm(lab+1)
+        for (int idx = lane; idx < ncd * nh1; idx += 32) {
+          const int cd = idx / nh1, h = idx % nh1;
+          int t, u, v, cx, cy, cz, dx, dy, dz;
+          wherm(h, t, u, v);
+          wcart(lc, cd / nd, cx, cy, cz);
+          wcart(ld, cd % nd, dx, dy, dz);
+          double x = 0.0;
+          for (int tp = 0; tp <= cx + dx; ++tp)
+            for (int up = 0; up <= cy + dy; ++up) {
+              const double fxy = sm->Fk[0][cx][dx][tp] * sm->Fk[1][cy][dy][up];
+              for (int vp = 0; vp <= cz + dz; ++vp)
+                x += fxy * sm->Fk[2][cz][dz][vp] * sm->R[herm_index(t + tp, u + up, v + vp)];
+            }
+          sm->X[idx] = x;
+        }
+        __syncwarp();
+        // bra derivatives (A, B)
+        for (int e = lane; e < ntot; e += 32) {
+          const double w = sm->G[e];
+          if (w == 0.0) continue;
+          const int ab = e / ncd, cd = e % ncd;
+          int ax, ay, az, bx, by, bz;
+          wcart(la, ab / nb, ax, ay, az);
+          wcart(lb, ab % nb, bx, by, bz);
+          const double* Xc = sm->X + cd * nh1;
+          double s[6] = {0, 0, 0, 0, 0, 0};
+          for (int t = 0; t <= ax + bx + 1; ++t)
+            for (int u = 0; u <= ay + by + 1; ++u)
+              for (int v = 0; v <= az + bz + 1; ++v) {
+                const double xv = Xc[herm_index(t, u, v)];
+                const double ex = t <= ax + bx ? sm->Eb[0][ax][bx][t] : 0.0;
+                const double ey = u <= ay + by ? sm->Eb[1][ay][by][u] : 0.0;
+                const double ez = v <= az + bz ? sm->Eb[2][az][bz][v] : 0.0;
+                // exactly one axis may exceed its plain range
+                const int over = (t > ax + bx) + (u > ay + by) + (v > az + bz);
+                if (over > 1) continue;
+                if (u <= ay + by && v <= az + bz) {
+                  s[0] += sm->DA[0][ax][bx][t] * ey * ez * xv;
+                  s[3] += sm->DB[0][ax][bx][t] * ey * ez * xv;
+                }
+                if (t <= ax + bx && v <= az + bz) {
+                  s[1] += ex * sm->DA[1][ay][by][u] * ez * xv;
+                  s[4] += ex * sm->DB[1][ay][by][u] * ez * xv;
+                }
+                if (t <= ax + bx && u <= ay + by) {
+                  s[2] += ex * ey * sm->DA[2][az][bz][v] * xv;
+                  s[5] += ex * ey * sm->DB[2][az][bz][v] * xv;
+                }
+              }
+          for (int k = 0; k < 6; ++k) g[k] += w * s[k];
+        }
+        // ket derivative (C), one axis at a time
+        for (int dir = 0; dir < 3; ++dir) {
+          __syncwarp();
+          for (int idx = lane; idx < ncd * nh0; idx += 32) {
+            const int cd = idx / nh0, h = idx % nh0;
+            int t, u, v, cx, cy, cz, dx, dy, dz;
+            wherm(h, t, u, v);
+            wcart(lc, cd / nd, cx, cy, cz);
+            wcart(ld, cd % nd, dx, dy, dz);
+            const int tx = cx + dx + (dir == 0), ty = cy + dy + (dir == 1), tz = cz + dz + (dir == 2);
+            double x = 0.0;
+            for (int tp = 0; tp <= tx; ++tp)
+              for (int up = 0; up <= ty; ++up)
+                for (int vp = 0; vp <= tz; ++vp) {
+                  const double fx = dir == 0 ? sm->DC[0][cx][dx][tp] : (tp <= cx + dx ? sm->Fk[0][cx][dx][tp] : 0.0);
+                  const double fy = dir == 1 ? sm->DC[1][cy][dy][up] : (up <= cy + dy ? sm->Fk[1][cy][dy][up] : 0.0);
+                  const double fz = dir == 2 ? sm->DC[2][cz][dz][vp] : (vp <= cz + dz ? sm->Fk[2][cz][dz][vp] : 0.0);
+                  x += fx * fy * fz * sm->R[herm_index(t + tp, u + up, v + vp)];
+                }
+            sm->X[idx] = x;
+          }
+          __syncwarp();
+          for (int e = lane; e < ntot; e += 32) {
+            const double w = sm->G[e];
+            if (w == 0.0) continue;
+            const int ab = e / ncd, cd = e % ncd;
+            int ax, ay, az, bx, by, bz;
+            wcart(la, ab / nb, ax, ay, az);
+            wcart(lb, ab % nb, bx, by, bz);
+            const double* Xc = sm->X + cd * nh0;
+            double s = 0.0;
+            for (int t = 0; t <= ax + bx; ++t)
+              for (int u = 0; u <= ay + by; ++u) {
+                const double exy = sm->Eb[0][ax][bx][t] * sm->Eb[1][ay][by][u];
+                for (int v = 0; v <= az + bz; ++v) s += exy * sm->Eb[2][az][bz][v] * Xc[herm_index(t, u, v)];
+              }
+            g[6 + dir] += w * s;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // reduce over the warp and scatter to the four atoms
+    double sc = 4.0;
+    if (bp.diag) sc *= 0.5;
+    if (kp.diag) sc *= 0.5;
+    if (task.bra == kidx) sc *= 0.5;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double v = g[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      g[k] = v * sc;
+    }
+    if (lane == 0) {
+      double* gr = prm.grad;
+      const int at[3] = {prm.atom[bp.a], prm.atom[bp.b], prm.atom[kp.a]};
+      const int atD = prm.atom[kp.b];
+      for (int k = 0; k < 3; ++k) {
+        for (int c = 0; c < 3; ++c) atomicAdd(gr + 3 * at[c] + k, g[3 * c + k]);
+        atomicAdd(gr + 3 * atD + k, -(g[k] + g[3 + k] + g[6 + k]));
+      }
+    }
+  }
+}
+
+cudaError_t launch_warp_grad(int la, int lb, int lc, int ld, const GradParams& p, cudaStream_t s) {
+  if (p.n_tasks == 0) return cudaSuccess;
+  const size_t sm = sizeof(GradSmem);
+  cudaError_t e = cudaFuncSetAttribute(warp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  warp_grad_kernel<<<p.n_tasks, 32, sm, s>>>(p, la, lb, lc, ld);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// One-electron derivative terms, one thread per shell pair (a >= b):
+//   grad += sum_ab D_ab d(T+V)_ab/dR - W_ab dS_ab/dR
+// with d/dA from derivative E coefficients (A-side 2 alpha E_{i+1} - i E_{i-1}),
+// d/dB = -d/dA for S and T, and for V the operator-centre term
+// dV/dC_x = -Z_C (2 pi/p) K sum E E E (-R_{t+1,u,v}) (Hellmann-Feynman) and
+// dV/dB = -dV/dA - sum_C dV/dC.
+__global__ void grad1e_kernel(const Grad1Params p) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npair = p.n_shell * (p.n_shell + 1) / 2;
+  if (idx >= npair) return;
+  int i = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
+  while (i * (i + 1) / 2 > idx) --i;
+  while ((i + 1) * (i + 2) / 2 <= idx) ++i;
+  const int j = idx - i * (i + 1) / 2;
+  const double fac = (i == j) ? 1.0 : 2.0;
+  const int la = p.l[i], lb = p.l[j];
+  const int na = ncart(la), nb = ncart(lb);
+  const double* A = p.centres + 3 * i;
+  const double* B = p.centres + 3 * j;
+  const int a0 = p.ao[i], b0 = p.ao[j];
+  const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+  double gA[3] = {0, 0, 0};   // d/dA of D(T+V) - W S
+  double gCs[3] = {0, 0, 0};  // sum over nuclei C of D dV/dC (for dV/dB)
+  for (int ia = 0; ia < p.nprim[i]; ++ia)
+    for (int ib = 0; ib < p.nprim[j]; ++ib) {
+      const double al = p.exps[p.prim_off[i] + ia], be = p.exps[p.prim_off[j] + ib];
+      const double w = p.coefs[p.prim_off[i] + ia] * p.coefs[p.prim_off[j] + ib];
+      const double pp = al + be;
+      const double P[3] = {(al * A[0] + be * B[0]) / pp, (al * A[1] + be * B[1]) / pp, (al * A[2] + be * B[2]) / pp};
+      const double K = exp(-(al * be / pp) * ab2) * w;
+      const double inv2p = 0.5 / pp;
+      // E up to (la+2, lb+1) per axis: dims [5][4][8]
+      double E[3][5][4][8];
+      double S1[3][5][4], T1[3][4][3];
+      for (int x = 0; x < 3; ++x) {
+        const double pa = P[x] - A[x], pb = P[x] - B[x];
+        for (int a = 0; a <= la + 2; ++a)
+          for (int b = 0; b <= lb + 1; ++b)
+            for (int tt = 0; tt < 8; ++tt) E[x][a][b][tt] = 0.0;
+        E[x][0][0][0] = 1.0;
+        for (int a = 0; a < la + 2; ++a)
+          for (int tt = 0; tt <= a + 1; ++tt) {
+            double val = 0.0;
+            if (tt <= a) val = pa * E[x][a][0][tt];
+            if (tt >= 1) val += inv2p * E[x][a][0][tt - 1];
+            if (tt + 1 <= a) val += (tt + 1) * E[x][a][0][tt + 1];
+            E[x][a + 1][0][tt] = val;
+          }
+        for (int b = 0; b < lb + 1; ++b)
+          for (int a = 0; a <= la + 2; ++a)
+            for (int tt = 0; tt <= a + b + 1; ++tt) {
+              double val = 0.0;
+              if (tt <= a + b) val = pb * E[x][a][b][tt];
+              if (tt >= 1) val += inv2p * E[x][a][b][tt - 1];
+              if (tt + 1 <= a + b) val += (tt + 1) * E[x][a][b][tt + 1];
+              E[x][a][b + 1][tt] = val;
+            }
+        const double sq = sqrt(M_PI / pp);
+        for (int a = 0; a <= la + 2; ++a)
+          for (int b = 0; b <= lb + 1; ++b) S1[x][a][b] = sq * E[x][a][b][0];
+        for (int a = 0; a <= la + 1; ++a)
+          for (int b = 0; b <= lb; ++b) {
+            double tv = 4.0 * al * be * S1[x][a + 1][b + 1];
+            if (a > 0 && b > 0) tv += a * b * S1[x][a - 1][b - 1];
+            if (b > 0) tv -= 2.0 * al * b * S1[x][a + 1][b - 1];
+            if (a > 0) tv -= 2.0 * be * a * S1[x][a - 1][b + 1];
+            T1[x][a][b] = 0.5 * tv;
+          }
+      }
+      // overlap and kinetic derivatives w.r.t. A
+      for (int a = 0; a < na; ++a)
+        for (int b = 0; b < nb; ++b) {
+          int ac[3], bc[3];
+          wcart(la, a, ac[0], ac[1], ac[2]);
+          wcart(lb, b, bc[0], bc[1], bc[2]);
+          const double dv = p.D[(size_t)(a0 + a) * p.n + b0 + b];
+          const double wv = p.W[(size_t)(a0 + a) * p.n + b0 + b];
+          double s[3], tk[3], ds[3], dt[3];
+          for (int x = 0; x < 3; ++x) {
+            s[x] = S1[x][ac[x]][bc[x]];
+            tk[x] = T1[x][ac[x]][bc[x]];
+            ds[x] = 2.0 * al * S1[x][ac[x] + 1][bc[x]] - (ac[x] > 0 ? ac[x] * S1[x][ac[x] - 1][bc[x]] : 0.0);
+            dt[x] = 2.0 * al * T1[x][ac[x] + 1][bc[x]] - (ac[x] > 0 ? ac[x] * T1[x][ac[x] - 1][bc[x]] : 0.0);
+          }
+          for (int x = 0; x < 3; ++x) {
+            const int y = (x + 1) % 3, z = (x + 2) % 3;
+            const double dS = K * ds[x] * s[y] * s[z];
+            const double dT = K * (dt[x] * s[y] * s[z] + ds[x] * (tk[y] * s[z] + s[y] * tk[z]));
+            gA[x] += dv * dT - wv * dS;
+          }
+        }
+      // nuclear attraction: d/dA (operator fixed) and d/dC (operator centre)
+      const int L = la + lb + 1;
+      for (int c = 0; c < p.n_atom; ++c) {
+        const double X = P[0] - p.atom_xyz[3 * c], Y = P[1] - p.atom_xyz[3 * c + 1], Z = P[2] - p.atom_xyz[3 * c + 2];
+        double F[kBoysMaxM + 1];
+        boys_eval_rt<double>(pp * (X * X + Y * Y + Z * Z), p.boys, L, F);
+        const double pref = -p.atom_Z[c] * (2.0 * M_PI / pp) * K;
+        double R[nherm(5)];
+        double Rn[6];
+        double pw = pref;
+        for (int m = 0; m <= L; ++m) {
+          Rn[m] = pw * F[m];
+          pw *= -2.0 * pp;
+        }
+        R[0] = Rn[L];
+        for (int m = L - 1; m >= 0; --m) {
+          for (int sh = L - m; sh >= 1; --sh) {
+            const int base = sh * (sh + 1) * (sh + 2) / 6;
+            for (int k = 0; k < ncart(sh); ++k) {
+              int tt, u, vv;
+              wcart(sh, k, tt, u, vv);
+              double val;
+              if (tt > 0) {
+                val = X * R[herm_index(tt - 1, u, vv)];
+                if (tt > 1) val += (tt - 1) * R[herm_index(tt - 2, u, vv)];
+              } else if (u > 0) {
+                val = Y * R[herm_index(tt, u - 1, vv)];
+                if (u > 1) val += (u - 1) * R[herm_index(tt, u - 2, vv)];
+              } else {
+                val = Z * R[herm_index(tt, u, vv - 1)];
+                if (vv > 1) val += (vv - 1) * R[herm_index(tt, u, vv - 2)];
+              }
+              R[base + k] = val;
+            }
+          }
+          R[0] = Rn[m];
+        }
+        double gC[3] = {0, 0, 0};
+        for (int a = 0; a < na; ++a)
+          for (int b = 0; b < nb; ++b) {
+            int ac[3], bc[3];
+            wcart(la, a, ac[0], ac[1], ac[2]);
+            wcart(lb, b, bc[0], bc[1], bc[2]);
+            const double dv = p.D[(size_t)(a0 + a) * p.n + b0 + b];
+            for (int x = 0; x < 3; ++x) {
+              const int y = (x + 1) % 3, z = (x + 2) % 3;
+              // A derivative: DE along x
+              double accA = 0.0, accC = 0.0;
+              for (int t0 = 0; t0 <= ac[x] + bc[x] + 1; ++t0) {
+                double de = 2.0 * al * E[x][ac[x] + 1][bc[x]][t0];
+                if (ac[x] > 0) de -= ac[x] * E[x][ac[x] - 1][bc[x]][t0];
+                const double e0 = t0 <= ac[x] + bc[x] ? E[x][ac[x]][bc[x]][t0] : 0.0;
+                for (int u0 = 0; u0 <= ac[y] + bc[y]; ++u0)
+                  for (int v0 = 0; v0 <= ac[z] + bc[z]; ++v0) {
+                    int h[3];
+                    h[x] = t0;
+                    h[y] = u0;
+                    h[z] = v0;
+                    const double eyz = E[y][ac[y]][bc[y]][u0] * E[z][ac[z]][bc[z]][v0];
+                    accA += de * eyz * R[herm_index(h[0], h[1], h[2])];
+                    if (t0 <= ac[x] + bc[x]) {
+                      int g1[3] = {h[0], h[1], h[2]};
+                      g1[x] += 1;
+                      accC -= e0 * eyz * R[herm_index(g1[0], g1[1], g1[2])];
+                    }
+                  }
+              }
+              gA[x] += dv * accA;
+              gC[x] += dv * accC;
+            }
+          }
+        for (int x = 0; x < 3; ++x) {
+          atomicAdd(p.grad + 3 * c + x, fac * gC[x]);
+          gCs[x] += gC[x];
+        }
+      }
+    }
+  // S and T: d/dB = -d/dA; V: d/dB = -d/dA - sum_C d/dC.
+  const int atA = p.atom[i], atB = p.atom[j];
+  for (int x = 0; x < 3; ++x) {
+    atomicAdd(p.grad + 3 * atA + x, fac * gA[x]);
+    atomicAdd(p.grad + 3 * atB + x, -fac * (gA[x] + gCs[x]));
+  }
+}
+
+cudaError_t launch_grad1e(const Grad1Params& p, cudaStream_t s) {
+  const int npair = p.n_shell * (p.n_shell + 1) / 2;
+  if (npair == 0) return cudaSuccess;
+  grad1e_kernel<<<(npair + 63) / 64, 64, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace jqc

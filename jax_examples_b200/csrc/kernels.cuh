@@ -87,6 +87,43 @@ __host__ __device__ constexpr int qc_L(int qc) {
 // warp engine.
 __host__ __device__ constexpr bool is_reg_class(int qc) { return qc_L(qc) <= 6; }
 
+struct GradParams {
+  const Task* tasks;
+  int n_tasks;
+  const ShellPair* pairs;
+  const PrimPair* pp;
+  const double* centres;
+  const int* ao;
+  const int* atom;        // atom of each shell
+  const double* boys;
+  const double* D;        // n_dens x n x n
+  int n_dens;
+  int n;
+  double jscale, kscale;
+  double* grad;           // n_atom x 3 (accumulated)
+};
+
+struct Grad1Params {
+  int n_shell, n, n_atom;
+  const int* l;
+  const int* nprim;
+  const int* prim_off;
+  const double* exps;
+  const double* coefs;
+  const double* centres;
+  const int* ao;
+  const int* atom;
+  const double* atom_xyz;
+  const double* atom_Z;
+  const double* boys;
+  const double* D;
+  const double* W;
+  double* grad;
+};
+
+cudaError_t launch_warp_grad(int la, int lb, int lc, int ld, const GradParams& p, cudaStream_t s);
+cudaError_t launch_grad1e(const Grad1Params& p, cudaStream_t s);
+
 cudaError_t launch_warp_jk(int la, int lb, int lc, int ld, bool fp32, const JKParams& p, cudaStream_t s);
 cudaError_t launch_warp_tensor(int la, int lb, int lc, int ld, const TensorParams& p, cudaStream_t s);
 cudaError_t launch_warp_schwarz(int la, int lb, const SchwarzParams& p, cudaStream_t s);

@@ -1,0 +1,80 @@
+"""Analytic nuclear gradients (ERI-derivative adjoint + one-electron terms)
+against the reference's finite-difference gradient (golden), the oracle's
+restatement of it, and central differences of the total energy."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from jax_examples_b200 import CalcConfig, compute_integrals, run_scf
+from jax_examples_b200 import basis as pb
+from jax_examples_b200.core import make_molecule
+from jax_examples_b200.grad import numerical_gradient, rhf_gradient, uhf_gradient
+
+pytestmark = pytest.mark.gpu
+
+
+def _scf(mol, bs, **kw):
+    ints = compute_integrals(mol, bs, device=0, schwarz_tau=kw.pop("tau", 0.0))
+    return run_scf(mol, ints, CalcConfig(method="uhf" if mol.spin else "rhf", scf_conv=1e-11, **kw))
+
+
+def test_rhf_gradient_vs_reference_golden(golden):
+    g = golden("water_synsto3g")
+    mol, bs = g.molecule(), g.basis()
+    res = _scf(mol, bs)
+    grad = rhf_gradient(mol, res).cpu().numpy()
+    np.testing.assert_allclose(grad, g.arr["grad"], atol=1e-7)
+    # translational invariance
+    np.testing.assert_allclose(grad.sum(axis=0), 0.0, atol=1e-9)
+
+
+def test_rhf_gradient_d_shells_vs_oracle_fd():
+    mol = pb.water_cluster(1)
+    build = lambda m: pb.build_basis_set(m, "syn-6-31g*")  # noqa: E731
+    bs = build(mol)
+    res = _scf(mol, bs)
+    grad = rhf_gradient(mol, res).cpu().numpy()
+    E, D, C, eps, ok = oracle.rhf_energy(mol, build, mode=1, conv=1e-11)
+    ref = oracle.rhf_gradient_fd(mol, build, D, C, eps, mode=1,
+                                 displace=lambda m, c: make_molecule(m.elements, c, m.atomic_numbers, m.charge, m.spin))
+    np.testing.assert_allclose(grad, ref, atol=1e-7)
+
+
+def test_autograd_matches_direct():
+    mol = pb.water_cluster(2, seed=4)
+    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    res = _scf(mol, bs, tau=1e-13)
+    g1 = rhf_gradient(mol, res).cpu().numpy()
+    g2 = rhf_gradient(mol, res, autograd=True).cpu().numpy()
+    np.testing.assert_allclose(g1, g2, atol=1e-12)
+
+
+def test_rhf_gradient_vs_energy_fd_dimer():
+    mol = pb.water_cluster(2, seed=2)
+    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    res = _scf(mol, bs, tau=1e-14)
+    grad = rhf_gradient(mol, res).cpu().numpy()
+    rng = np.random.default_rng(0)
+    h = 1e-4
+    for _ in range(3):
+        a, k = int(rng.integers(0, 6)), int(rng.integers(0, 3))
+        e = []
+        for sgn in (1, -1):
+            c = np.array(mol.coords, dtype=float)
+            c[a, k] += sgn * h
+            m = make_molecule(mol.elements, c, mol.atomic_numbers)
+            e.append(_scf(m, pb.build_basis_set(m, "syn-6-31g*"), tau=1e-14).energy)
+        assert abs((e[0] - e[1]) / (2 * h) - grad[a, k]) < 2e-6
+
+
+def test_uhf_gradient_vs_numerical(golden):
+    g = golden("water_cation_synsto3g_uhf")
+    mol, bs = g.molecule(), g.basis()
+    res = _scf(mol, bs)
+    grad = uhf_gradient(mol, res).cpu().numpy()
+    num = numerical_gradient(mol, "syn-sto-3g", step_size=1e-4, scf_conv=1e-11, device=0).numpy()
+    np.testing.assert_allclose(grad, num, atol=2e-6)
