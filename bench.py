@@ -38,11 +38,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_WATERS = 16
+N_WATERS = int(os.environ.get("JQC_BENCH_WATERS", "16"))
 BASIS = "syn-6-31g*"
 SCHWARZ_TAU = 1e-12
 METRIC = "ERI quartets/s (direct J/K Fock build, (H2O)16 6-31G*-shaped)"
-WORKLOAD = "(H2O)16 lattice 2.9A, 6-31G*-shaped Cartesian (304 bf), FP64 direct J/K build"
+WORKLOAD = (f"(H2O){N_WATERS} lattice 2.9A, 6-31G*-shaped Cartesian ({19 * N_WATERS} bf), "
+            "FP64 direct J/K build")
 
 
 def _dist():
@@ -288,7 +289,21 @@ def run_ours(args):
         rmx = run_scf(mol, ints, cfg)
         torch.cuda.synchronize()
         tmx = time.perf_counter() - t0
+        from jax_examples_b200.grad import rhf_gradient
+
+        rhf_gradient(mol, r64, engine=eng)  # warm-up (builds the gradient work list)
+        torch.cuda.synchronize()
+        ge0 = torch.cuda.Event(enable_timing=True)
+        ge1 = torch.cuda.Event(enable_timing=True)
+        ge0.record()
+        g64 = rhf_gradient(mol, r64, engine=eng)
+        ge1.record()
+        torch.cuda.synchronize()
+        tgrad = ge0.elapsed_time(ge1) * 1e-3
+        gmx = rhf_gradient(mol, rmx, engine=eng)
         fg = {"plain_fp64_scf_s": round(t64, 4), "plain_fp64_fock_s": round(r64.precision["jk_seconds"], 4),
+              "gradient_s": round(tgrad, 4),
+              "gradient_err_eh_bohr": float((g64 - gmx).abs().max()),
               "plain_iterations": r64.n_iterations, "chosen_scf_s": round(tmx, 4),
               "chosen_fock_s": round(rmx.precision["jk_seconds"], 4), "chosen_iterations": rmx.n_iterations,
               "chosen_builds": {k: rmx.precision[k] for k in ("builds_mixed", "builds_fp64", "incremental_builds")},
@@ -339,7 +354,12 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-scf", dest="scf", action="store_false")
+    ap.add_argument("--waters", type=int, default=None, help="cluster size (default 16; profiling uses smaller)")
     args = ap.parse_args()
+    if args.waters is not None:
+        global N_WATERS, WORKLOAD
+        N_WATERS = args.waters
+        WORKLOAD = WORKLOAD.replace("(H2O)16", f"(H2O){N_WATERS}").replace("(304 bf)", f"({19 * N_WATERS} bf)")
     if args.impl == "reference":
         run_reference(args)
     else:

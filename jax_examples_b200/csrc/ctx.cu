@@ -269,7 +269,7 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
         if (!full && !grad) chunk = std::max(1, std::min(nbp, kMaxLanePrims / std::max(1, nkp)));
         // Register classes: 32 kets per warp task (one per lane).  Warp-engine
         // classes: one ket per task, so every quartet gets its own warp.
-        const int per_task = (is_reg_class(qc) && !grad) ? 32 : 1;
+        const int per_task = grad ? (is_grad_reg_class(qc) ? 32 : 1) : (is_reg_class(qc) ? 32 : 1);
         for (int prec = 0; prec < 2; ++prec) {
           for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
             for (int b0 = 0; b0 < nbp; b0 += chunk) {
@@ -758,7 +758,10 @@ int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k
     p.kscale = k_scale;
     p.grad = grad;
     const int pb = qc_bra(qc), pk = qc_ket(qc);
-    JQC_CUDA_CHECK(launch_warp_grad(pc_la(pb), pc_lb(pb), pc_la(pk), pc_lb(pk), p, s));
+    if (is_grad_reg_class(qc))
+      JQC_CUDA_CHECK(launch_grad_reg(qc, p, s));
+    else
+      JQC_CUDA_CHECK(launch_warp_grad(pc_la(pb), pc_lb(pb), pc_la(pk), pc_lb(pk), p, s));
   }
   return JQC_OK;
 }

@@ -121,6 +121,10 @@ struct Grad1Params {
   double* grad;
 };
 
+// Gradient classes evaluated by the register kernels (L <= 4); the rest use
+// the warp-cooperative gradient kernel.
+__host__ __device__ constexpr bool is_grad_reg_class(int qc) { return qc_L(qc) <= 4; }
+cudaError_t launch_grad_reg(int qc, const GradParams& p, cudaStream_t s);
 cudaError_t launch_warp_grad(int la, int lb, int lc, int ld, const GradParams& p, cudaStream_t s);
 cudaError_t launch_grad1e(const Grad1Params& p, cudaStream_t s);
 
