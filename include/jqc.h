@@ -60,9 +60,11 @@ int jqc_basis_upload(jqc_ctx *ctx, int n_shell, const int *l, const int *nprim, 
 
 /* Build shell-pair data (Gaussian products, E-coefficient inputs) and the
  * Schwarz bounds Q_ij = sqrt(max (ij|ij)) on the device; drop pairs that can
- * never pass Q_ij * max Q >= schwarz_tau.  Synchronizes `stream`.
+ * never pass Q_ij * max Q >= schwarz_tau, and primitive pairs whose
+ * magnitude |K_AB c_a c_b| pi^(5/4) p^(-5/4) is below prim_tau (0 keeps all).
+ * Synchronizes `stream`.
  * Replaces integrals/screening.py:32-58 (compute_shell_pair_bounds). */
-int jqc_pairs_build(jqc_ctx *ctx, double schwarz_tau, void *stream);
+int jqc_pairs_build(jqc_ctx *ctx, double schwarz_tau, double prim_tau, void *stream);
 
 /* Counters of the work list for (precision_mode, mixed_tau) as jqc_jk
  * would use it: out[0] shell pairs, out[1] kept pairs, out[2] screened

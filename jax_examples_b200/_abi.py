@@ -55,7 +55,7 @@ SIGNATURES = {
     "jqc_ctx_create": (_c_int, [_c_int, ctypes.POINTER(_vp)]),
     "jqc_ctx_destroy": (_c_int, [_vp]),
     "jqc_basis_upload": (_c_int, [_vp, _c_int, _ip, _ip, _ip, _dp, _dp, _dp, _ip, _c_int, _dp, _dp, _c_int]),
-    "jqc_pairs_build": (_c_int, [_vp, _c_dbl, _vp]),
+    "jqc_pairs_build": (_c_int, [_vp, _c_dbl, _c_dbl, _vp]),
     "jqc_stats": (_c_int, [_vp, _c_int, _c_dbl, _llp]),
     "jqc_schwarz": (_c_int, [_vp, _vp, _vp]),
     "jqc_boys": (_c_int, [_vp, _c_ll, _c_int, _vp, _c_int, _vp]),

@@ -36,17 +36,35 @@ __device__ __forceinline__ float boys_sqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ int boys_round(double x) { return __double2int_rn(x); }
 __device__ __forceinline__ int boys_round(float x) { return __float2int_rn(x); }
 
-// Writes F_0 .. F_M at T into F[0..M].  `tab` is the table for type T.
+// Aligned per-order table used by the hot kernels: for order M and grid
+// point i the 8 values F_{M+k}(T_i), k < 8, are one 64-byte (FP64) or 32-byte
+// (FP32) aligned row at tabA[(M * kBoysRows + i) * 8], fetched with 16-byte
+// vector loads.
+constexpr int kBoysARow = 8;
+
+__device__ __forceinline__ void boys_row(const double* __restrict__ r, double (&v)[8]) {
+  const double2* q = reinterpret_cast<const double2*>(r);
+  const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+}
+__device__ __forceinline__ void boys_row(const float* __restrict__ r, float (&v)[8]) {
+  const float4* q = reinterpret_cast<const float4*>(r);
+  const float4 a = __ldg(q), b = __ldg(q + 1);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+
+// Writes F_0 .. F_M at T into F[0..M] from the aligned table `tabA`.
 template <typename T, int M>
-__device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tab, T (&F)[M + 1]) {
+__device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F)[M + 1]) {
   constexpr int KT = BoysConst<T>::kTaylor;
   if (t < T(kBoysTMax)) {
     const int i = boys_round(t * T(kBoysGridInv));
     const T d = T(i) * T(1.0 / kBoysGridInv) - t;  // T_i - t
-    const T* row = tab + i * kBoysCols + M;
-    T acc = __ldg(row + KT - 1);
+    T v[8];
+    boys_row(tabA + (M * kBoysRows + i) * kBoysARow, v);
+    T acc = v[KT - 1];
 #pragma unroll
-    for (int k = KT - 2; k >= 0; --k) acc = __ldg(row + k) + acc * (d * T(1.0 / (k + 1)));
+    for (int k = KT - 2; k >= 0; --k) acc = v[k] + acc * (d * T(1.0 / (k + 1)));
     F[M] = acc;
     if (M > 0) {
       const T e = boys_exp(-t);
@@ -90,8 +108,17 @@ __device__ __forceinline__ void boys_eval_rt(T t, const T* __restrict__ tab, int
 // Host: fill the FP64 table (kBoysRows * kBoysCols) in long double.
 void boys_fill_table(double* tab);
 
-// Per-device lazily created tables (device pointers).  The first call on a
-// device allocates and uploads them; later calls return the cached pointers.
+// Per-device lazily created tables (device pointers): the row-major base
+// table (kBoysRows x kBoysCols) and the aligned per-order table
+// ((kBoysMaxM+1) x kBoysRows x 8), FP64 and FP32.  The first call on a device
+// allocates and uploads them; later calls return the cached pointers.
+struct BoysTables {
+  const double* t64;
+  const float* t32;
+  const double* a64;
+  const float* a32;
+};
 int boys_tables(int device, const double** d64, const float** d32);
+int boys_tables_all(int device, BoysTables* out);
 
 }  // namespace jqc

@@ -108,37 +108,51 @@ void boys_fill_table(double* tab) {
   }
 }
 
-int boys_tables(int device, const double** d64, const float** d32) {
+int boys_tables_all(int device, BoysTables* out) {
   static std::mutex mu;
-  static std::vector<double*> t64;
-  static std::vector<float*> t32;
+  static std::vector<BoysTables> tabs;
   std::lock_guard<std::mutex> lock(mu);
   int ndev = 0;
   JQC_CUDA_CHECK(cudaGetDeviceCount(&ndev));
   JQC_REQUIRE(device >= 0 && device < ndev, JQC_ERR_INVALID, "invalid CUDA device");
-  if ((int)t64.size() < ndev) {
-    t64.resize(ndev, nullptr);
-    t32.resize(ndev, nullptr);
-  }
-  if (!t64[device]) {
+  if ((int)tabs.size() < ndev) tabs.resize(ndev, BoysTables{nullptr, nullptr, nullptr, nullptr});
+  if (!tabs[device].t64) {
     std::vector<double> h(kBoysRows * kBoysCols);
     boys_fill_table(h.data());
     std::vector<float> hf(h.begin(), h.end());
+    const size_t na = (size_t)(kBoysMaxM + 1) * kBoysRows * kBoysARow;
+    std::vector<double> ha(na);
+    for (int M = 0; M <= kBoysMaxM; ++M)
+      for (int i = 0; i < kBoysRows; ++i)
+        for (int k = 0; k < kBoysARow; ++k)
+          ha[((size_t)M * kBoysRows + i) * kBoysARow + k] = h[(size_t)i * kBoysCols + M + k];
+    std::vector<float> haf(ha.begin(), ha.end());
     int prev = 0;
     JQC_CUDA_CHECK(cudaGetDevice(&prev));
     JQC_CUDA_CHECK(cudaSetDevice(device));
-    double* p64 = nullptr;
-    float* p32 = nullptr;
+    double *p64 = nullptr, *a64 = nullptr;
+    float *p32 = nullptr, *a32 = nullptr;
     JQC_CUDA_CHECK(cudaMalloc(&p64, h.size() * sizeof(double)));
     JQC_CUDA_CHECK(cudaMalloc(&p32, hf.size() * sizeof(float)));
+    JQC_CUDA_CHECK(cudaMalloc(&a64, ha.size() * sizeof(double)));
+    JQC_CUDA_CHECK(cudaMalloc(&a32, haf.size() * sizeof(float)));
     JQC_CUDA_CHECK(cudaMemcpy(p64, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
     JQC_CUDA_CHECK(cudaMemcpy(p32, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    JQC_CUDA_CHECK(cudaMemcpy(a64, ha.data(), ha.size() * sizeof(double), cudaMemcpyHostToDevice));
+    JQC_CUDA_CHECK(cudaMemcpy(a32, haf.data(), haf.size() * sizeof(float), cudaMemcpyHostToDevice));
     JQC_CUDA_CHECK(cudaSetDevice(prev));
-    t64[device] = p64;
-    t32[device] = p32;
+    tabs[device] = BoysTables{p64, p32, a64, a32};
   }
-  *d64 = t64[device];
-  *d32 = t32[device];
+  *out = tabs[device];
+  return JQC_OK;
+}
+
+int boys_tables(int device, const double** d64, const float** d32) {
+  BoysTables t;
+  int rc = boys_tables_all(device, &t);
+  if (rc) return rc;
+  *d64 = t.t64;
+  *d32 = t.t32;
   return JQC_OK;
 }
 
@@ -201,10 +215,17 @@ struct jqc_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join[kNumStreams] = {};
   const double* boys64 = nullptr;
   const float* boys32 = nullptr;
+  const double* boysA64 = nullptr;  // aligned per-order tables (hot kernels)
+  const float* boysA32 = nullptr;
+  double prim_tau = 0.0;
 };
 
 namespace jqc {
 
+// Primitive pairs of shell pair (a, b).  A pair whose magnitude
+// |K_AB c_a c_b| pi^{5/4} p^{-5/4} (the s-type sqrt((ab|ab)) of the
+// primitive pair) is below prim_tau contributes nothing at that level to any
+// integral and is dropped.
 static void make_prim_pairs(const jqc_ctx* c, int a, int b, std::vector<PrimPair>& out) {
   const double* A = &c->centres[3 * a];
   const double* B = &c->centres[3 * b];
@@ -223,6 +244,8 @@ static void make_prim_pairs(const jqc_ctx* c, int a, int b, std::vector<PrimPair
       q.alpha = al;
       q.beta = be;
       q.h = 0.5 / p;
+      const double mag = std::fabs(q.K) * 4.1606878161 * std::pow(p, -1.25);  // pi^{5/4}
+      if (c->prim_tau > 0.0 && mag < c->prim_tau) continue;
       out.push_back(q);
     }
 }
@@ -377,11 +400,16 @@ int jqc_ctx_create(int device, jqc_ctx** out) {
   JQC_REQUIRE(device >= 0 && device < ndev, JQC_ERR_INVALID, "jqc_ctx_create: invalid device");
   jqc_ctx* c = new jqc_ctx();
   c->device = device;
-  int rc = boys_tables(device, &c->boys64, &c->boys32);
+  BoysTables bt;
+  int rc = boys_tables_all(device, &bt);
   if (rc != JQC_OK) {
     delete c;
     return rc;
   }
+  c->boys64 = bt.t64;
+  c->boys32 = bt.t32;
+  c->boysA64 = bt.a64;
+  c->boysA32 = bt.a32;
   cudaError_t e = cudaSetDevice(device);
   for (int i = 0; i < kNumStreams && e == cudaSuccess; ++i) {
     e = cudaStreamCreateWithFlags(&c->side[i], cudaStreamNonBlocking);
@@ -479,11 +507,13 @@ int jqc_basis_upload(jqc_ctx* c, int n_shell, const int* l, const int* nprim, co
   return JQC_OK;
 }
 
-int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
+int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, double prim_tau, void* stream) {
   JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_pairs_build: null context");
   JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_pairs_build: call jqc_basis_upload first");
   JQC_REQUIRE(schwarz_tau >= 0.0 && std::isfinite(schwarz_tau), JQC_ERR_INVALID,
               "jqc_pairs_build: schwarz_tau must be >= 0");
+  JQC_REQUIRE(prim_tau >= 0.0 && std::isfinite(prim_tau), JQC_ERR_INVALID, "jqc_pairs_build: prim_tau must be >= 0");
+  c->prim_tau = prim_tau;
   int rc = select_device(c);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -532,6 +562,7 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
     p.pp = d_rawpp.ptr;
     p.centres = c->d_centres.ptr;
     p.boys = c->boys64;
+    p.boys_al = c->boysA64;
     p.qmax = d_q.ptr;
     JQC_CUDA_CHECK(launch_schwarz(pc, p, s));
   }
@@ -555,7 +586,7 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
     if (raw[k].Q * qmax >= schwarz_tau && raw[k].Q > 0.0) keep.push_back((int)k);
   auto key = [&](int k) {
     const ShellPair& p = raw[k];
-    return std::make_tuple(p.cls, c->nprim[p.a], c->nprim[p.b]);
+    return std::make_tuple(p.cls, p.npp, 1);
   };
   std::stable_sort(keep.begin(), keep.end(), [&](int x, int y) {
     auto kx = key(x), ky = key(y);
@@ -573,8 +604,8 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, void* stream) {
     for (int k = 0; k < sp.npp; ++k) {
       const PrimPair& q = rawpp[src + k];
       pp.push_back(q);
-      ppf.push_back(PrimPairF{float(q.p), float(q.Px), float(q.Py), float(q.Pz), float(q.K), float(q.alpha),
-                              float(q.beta), float(q.h)});
+      ppf.push_back(PrimPairF{float(q.p), float(q.h), float(q.Px), float(q.Py), float(q.Pz), float(q.K),
+                              float(q.alpha), float(q.beta)});
     }
     auto kk = key(keep[r]);
     if (c->blocks.empty() || std::get<0>(kk) != c->blocks.back().pc || std::get<1>(kk) != c->blocks.back().ka ||
@@ -690,11 +721,10 @@ int jqc_eri_prim_quartets(int la, int lb, int lc, int ld, long long n, const dou
   JQC_REQUIRE(exps && centres && out, JQC_ERR_INVALID, "jqc_eri_prim_quartets: null pointer");
   int dev = 0;
   JQC_CUDA_CHECK(cudaGetDevice(&dev));
-  const double* t64;
-  const float* t32;
-  int rc = boys_tables(dev, &t64, &t32);
+  BoysTables bt;
+  int rc = boys_tables_all(dev, &bt);
   if (rc) return rc;
-  PrimQuartetParams p{n, exps, centres, t64, out};
+  PrimQuartetParams p{n, exps, centres, bt.t64, bt.a64, out};
   JQC_CUDA_CHECK(launch_prim_quartets(la, lb, lc, ld, p, static_cast<cudaStream_t>(stream)));
   return JQC_OK;
 }
@@ -720,6 +750,7 @@ int jqc_eri_tensor(jqc_ctx* c, double* out, long long max_bytes, void* stream) {
     p.centres = c->d_centres.ptr;
     p.ao = c->d_ao.ptr;
     p.boys = c->boys64;
+    p.boys_al = c->boysA64;
     p.eri = out;
     p.n = c->n_bf;
     JQC_CUDA_CHECK(launch_eri_tensor(qc, p, s));
@@ -751,6 +782,7 @@ int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k
     p.ao = c->d_ao.ptr;
     p.atom = c->d_atom.ptr;
     p.boys = c->boys64;
+    p.boys_al = c->boysA64;
     p.D = D;
     p.n_dens = n_dens;
     p.n = c->n_bf;
@@ -875,6 +907,7 @@ static int jk_impl(jqc_ctx* c, int n_dens, const double* D, double* J, double* K
       p.centres = c->d_centres.ptr;
       p.ao = c->d_ao.ptr;
       p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
+      p.boys_al = prec ? (const void*)c->boysA32 : (const void*)c->boysA64;
       p.D = D;
       p.J = J;
       p.K = K;
@@ -959,6 +992,7 @@ int jk_run_preallocated(jqc_ctx* c, int n_dens, const double* D, double* J, doub
       p.centres = c->d_centres.ptr;
       p.ao = c->d_ao.ptr;
       p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
+      p.boys_al = prec ? (const void*)c->boysA32 : (const void*)c->boysA64;
       p.D = D;
       p.J = J;
       p.K = K;

@@ -27,7 +27,7 @@ struct SchwarzBody {
     double out[Cfg::NAB][Cfg::CDP];
     double ebuf[3][LA + 1][LB + 1][LA + LB + 1];
     quartet_accumulate<double, LA, LB, LA, LB, NS, PART, false>(prm.pp + bp.pp, bp.npp, A, B, prm.pp + bp.pp,
-                                                                 bp.npp, A, B, prm.boys, ebuf, out);
+                                                                 bp.npp, A, B, prm.boys_al, ebuf, out);
     double m = 0.0;
     static_for<Cfg::NCDP>([&](auto c_) {
       constexpr int cdi = decltype(c_)::value;
@@ -87,18 +87,19 @@ struct PrimBody {
     {
       const double al = ex[0], be = ex[1], p = al + be;
       const double dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
-      bra = PrimPair{p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
-                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
+      bra = PrimPair{p, 0.5 / p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
+                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be};
     }
     {
       const double al = ex[2], be = ex[3], p = al + be;
       const double dx = C.x - D.x, dy = C.y - D.y, dz = C.z - D.z;
-      ket = PrimPair{p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
-                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
+      ket = PrimPair{p, 0.5 / p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
+                     exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be};
     }
     double out[Cfg::NAB][Cfg::CDP];
     double ebuf[3][LA + 1][LB + 1][LA + LB + 1];
-    quartet_accumulate<double, LA, LB, LC, LD, NS, PART, false>(&bra, 1, A, B, &ket, 1, C, D, prm.boys, ebuf, out);
+    quartet_accumulate<double, LA, LB, LC, LD, NS, PART, false, false>(&bra, 1, A, B, &ket, 1, C, D, prm.boys_al,
+                                                                        ebuf, out);
     double* o = prm.out + q * (Cfg::NAB * Cfg::NCD);
     static_for<Cfg::NAB * Cfg::NCDP>([&](auto x_) {
       constexpr int x = decltype(x_)::value;

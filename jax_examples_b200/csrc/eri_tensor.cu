@@ -33,7 +33,7 @@ struct TensorBody {
     Vec3<double> D{ctr[3 * kp.b], ctr[3 * kp.b + 1], ctr[3 * kp.b + 2]};
     double out[Cfg::NAB][Cfg::CDP];
     quartet_accumulate<double, LA, LB, LC, LD, NS, PART, true>(prm.pp + bp.pp, bp.npp, A, B, prm.pp + kp.pp,
-                                                                active ? kp.npp : 0, C, D, prm.boys, ebra, out);
+                                                                active ? kp.npp : 0, C, D, prm.boys_al, ebra, out);
     if (!active) return;
     const long long n = prm.n;
     const long long a0 = prm.ao[bp.a], b0 = prm.ao[bp.b], c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];

@@ -122,7 +122,7 @@ struct GradBody {
         ecoef_compute<double, LC + 1, LD, true>(F[1], kpp.Py - C.y, kpp.Py - Dc.y, kpp.h);
         ecoef_compute<double, LC + 1, LD, true>(F[2], kpp.Pz - C.z, kpp.Pz - Dc.z, kpp.h);
         double R[nherm(L + 1)];
-        prim_quartet_R<double, L + 1>(bpp, kpp, static_cast<const double*>(prm.boys), R);
+        prim_quartet_R<double, L + 1>(bpp, kpp, prm.boys_al, R);
         const double two_g = 2.0 * kpp.alpha;
 
         static_for<NCDP>([&](auto cdi_) {

@@ -74,7 +74,7 @@ struct JKBody {
     T out[Cfg::NAB][Cfg::CDP];
     const int p0 = task.flags & 0xffff, p1 = task.flags >> 16;  // bra primitive-pair range
     quartet_accumulate<T, LA, LB, LC, LD, NS, PART, true>(pp + bp.pp + p0, p1 - p0, A, B, pp + kp.pp,
-                                                           active ? kp.npp : 0, C, D, static_cast<const T*>(prm.boys),
+                                                           active ? kp.npp : 0, C, D, static_cast<const T*>(prm.boys_al),
                                                            ebra, out);
 
     double s = active ? 1.0 : 0.0;

@@ -20,7 +20,8 @@ struct JKParams {
   const void* pp;          // PrimPair* (FP64) or PrimPairF* (FP32)
   const double* centres;   // 3 per shell
   const int* ao;           // first basis function of each shell
-  const void* boys;        // Boys table of the kernel's type
+  const void* boys;        // Boys table of the kernel's type (row-major)
+  const void* boys_al;     // aligned per-order Boys table of the kernel's type
   const double* D;         // n_dens x n x n
   double* J;               // n_dens x n x n (accumulated, symmetrized later)
   double* K;
@@ -39,6 +40,7 @@ struct TensorParams {
   const double* centres;
   const int* ao;
   const double* boys;
+  const double* boys_al;
   double* eri;
   long long n;
 };
@@ -50,6 +52,7 @@ struct SchwarzParams {
   const PrimPair* pp;
   const double* centres;
   const double* boys;
+  const double* boys_al;
   unsigned long long* qmax;  // max (ab|ab) as ordered bits, per pair
 };
 
@@ -58,6 +61,7 @@ struct PrimQuartetParams {
   const double* exps;      // 4 per quartet
   const double* centres;   // 12 per quartet
   const double* boys;
+  const double* boys_al;
   double* out;             // n x (nab*ncd)
 };
 
@@ -96,6 +100,7 @@ struct GradParams {
   const int* ao;
   const int* atom;        // atom of each shell
   const double* boys;
+  const double* boys_al;
   const double* D;        // n_dens x n x n
   int n_dens;
   int n;

@@ -21,11 +21,25 @@ namespace jqc {
 // P = (alpha A + beta B) / p, K = exp(-alpha beta |AB|^2 / p) c_a c_b,
 // h = 1/(2p) (kept so no kernel divides by p).
 struct __align__(16) PrimPair {
-  double p, Px, Py, Pz, K, alpha, beta, h;
+  double p, h, Px, Py, Pz, K, alpha, beta;
 };
 struct __align__(16) PrimPairF {
-  float p, Px, Py, Pz, K, alpha, beta, h;
+  float p, h, Px, Py, Pz, K, alpha, beta;
 };
+
+// 16-byte vector loads of a primitive-pair record through the read-only path
+// (global memory only; records built in registers/local memory are read
+// with plain loads, see quartet_accumulate's GLOBAL_PP).
+__device__ __forceinline__ PrimPair ld_pp(const PrimPair* q) {
+  const double2* v = reinterpret_cast<const double2*>(q);
+  const double2 a = __ldg(v), b = __ldg(v + 1), c = __ldg(v + 2), d = __ldg(v + 3);
+  return PrimPair{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y};
+}
+__device__ __forceinline__ PrimPairF ld_pp(const PrimPairF* q) {
+  const float4* v = reinterpret_cast<const float4*>(q);
+  const float4 a = __ldg(v), b = __ldg(v + 1);
+  return PrimPairF{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+}
 template <typename T>
 struct PPType;
 template <>
@@ -188,7 +202,9 @@ __device__ __forceinline__ void prim_quartet_R(const PPT& bp, const PPT& kp, con
 // coefficients live in `ebra` (3 axes); with SHARED_BRA the bra pair is the
 // same for the whole warp, `ebra` is warp-private shared memory and lanes
 // 0..2 fill one axis each (every lane of the warp must call this function).
-template <typename T, int LA, int LB, int LC, int LD, int NS, int PART, bool SHARED_BRA>
+// GLOBAL_PP: bra/ket point into global memory (vector read-only loads);
+// false for primitive pairs built on the fly by the caller.
+template <typename T, int LA, int LB, int LC, int LD, int NS, int PART, bool SHARED_BRA, bool GLOBAL_PP = true>
 __device__ __forceinline__ void quartet_accumulate(
     const typename PPType<T>::type* __restrict__ bra, int nbra, Vec3<T> A, Vec3<T> B,
     const typename PPType<T>::type* __restrict__ ket, int nket, Vec3<T> C, Vec3<T> D,
@@ -203,7 +219,9 @@ __device__ __forceinline__ void quartet_accumulate(
   if constexpr (Cfg::NCDP > 0) {
     const int lane = threadIdx.x & 31;
     for (int ip = 0; ip < nbra; ++ip) {
-      const auto bp = bra[ip];
+      typename PPType<T>::type bp;
+      if constexpr (GLOBAL_PP) bp = ld_pp(bra + ip);
+      else bp = bra[ip];
       const T inv2p = bp.h;
       if constexpr (SHARED_BRA) {
         __syncwarp();
@@ -218,7 +236,9 @@ __device__ __forceinline__ void quartet_accumulate(
       }
       const EArr<T, LA, LB> Ex = ebra[0], Ey = ebra[1], Ez = ebra[2];
       for (int iq = 0; iq < nket; ++iq) {
-        const auto kp = ket[iq];
+        typename PPType<T>::type kp;
+        if constexpr (GLOBAL_PP) kp = ld_pp(ket + iq);
+        else kp = ket[iq];
         const T inv2q = kp.h;
         T fbuf[3][LC + 1][LD + 1][LC + LD + 1];
         ecoef_compute<T, LC, LD, true>(fbuf[0], kp.Px - C.x, kp.Px - D.x, inv2q);

@@ -202,14 +202,14 @@ __global__ void __launch_bounds__(kWarpBlock) warp_prim_kernel(const PrimQuartet
   {
     const double al = ex[0], be = ex[1], p = al + be;
     const double dx = A.x - B.x, dy = A.y - B.y, dz = A.z - B.z;
-    bra = PrimPair{p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
-                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
+    bra = PrimPair{p, 0.5 / p, (al * A.x + be * B.x) / p, (al * A.y + be * B.y) / p, (al * A.z + be * B.z) / p,
+                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be};
   }
   {
     const double al = ex[2], be = ex[3], p = al + be;
     const double dx = C.x - D.x, dy = C.y - D.y, dz = C.z - D.z;
-    ket = PrimPair{p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
-                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be, 0.5 / p};
+    ket = PrimPair{p, 0.5 / p, (al * C.x + be * D.x) / p, (al * C.y + be * D.y) / p, (al * C.z + be * D.z) / p,
+                   exp(-(al * be / p) * (dx * dx + dy * dy + dz * dz)), al, be};
   }
   WarpQuartet<double> wq;
   wq.sm = sm;

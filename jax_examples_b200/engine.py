@@ -92,9 +92,11 @@ class DirectERI:
             kernels; optional for pure two-electron use.
         device: CUDA device index (default: current).
         schwarz_tau: shell quartets with Q_ij Q_kl below this are skipped.
+        prim_tau: primitive pairs of magnitude below this are dropped
+            (1e-20 changes no integral by more than ~1e-19).
     """
 
-    def __init__(self, basis, mol=None, device=None, schwarz_tau: float = 1e-13):
+    def __init__(self, basis, mol=None, device=None, schwarz_tau: float = 1e-13, prim_tau: float = 1e-20):
         self.device = _require_cuda(device)
         self.lib = _abi.load()
         self.basis = basis
@@ -118,7 +120,7 @@ class DirectERI:
                 "jqc_basis_upload", self._ctx, pk.n_shell, ip(pk.l), ip(pk.nprim), ip(pk.prim_off), dp(pk.exps),
                 dp(pk.coefs), dp(pk.centres), ip(pk.atom), len(self.atom_Z), dp(self.atom_xyz), dp(self.atom_Z), 1,
             )
-            _abi.call("jqc_pairs_build", self._ctx, self.schwarz_tau, _stream(self.device))
+            _abi.call("jqc_pairs_build", self._ctx, self.schwarz_tau, float(prim_tau), _stream(self.device))
         self._C = None
         if pk.spherical:
             C = np.zeros((pk.n_basis, pk.n_cart))
