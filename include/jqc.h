@@ -66,6 +66,18 @@ int jqc_basis_upload(jqc_ctx *ctx, int n_shell, const int *l, const int *nprim, 
  * Replaces integrals/screening.py:32-58 (compute_shell_pair_bounds). */
 int jqc_pairs_build(jqc_ctx *ctx, double schwarz_tau, double prim_tau, void *stream);
 
+/* Batch partition: the uploaded atoms (and their shells) belong to n_mol
+ * independent molecules, mol_of_atom[a] in 0..n_mol-1.  Shell pairs, quartets,
+ * nuclear attraction and gradients then stay inside each molecule, and one
+ * jqc_jk / jqc_grad2e / jqc_one_electron call serves all molecules at once
+ * over one class-sorted work list (the basis-function matrices are the
+ * block-diagonal n x n matrices of the whole batch).  Call after
+ * jqc_basis_upload and before jqc_pairs_build; jqc_basis_upload resets it to
+ * one molecule.  Replaces the per-molecule loop of geomopt/optimizer.py:55-76
+ * (_energy_and_gradient per geometry): a sweep over many geometries or
+ * molecules is one call per step instead of one per molecule. */
+int jqc_batch_partition(jqc_ctx *ctx, int n_mol, const int *mol_of_atom);
+
 /* Counters of the work list for (precision_mode, mixed_tau) as jqc_jk
  * would use it: out[0] shell pairs, out[1] kept pairs, out[2] screened
  * canonical quartets on the FP64 path, out[3] on the FP32 path, out[4]
@@ -154,6 +166,45 @@ int jqc_jk_noalloc(jqc_ctx *ctx, int n_dens, const double *D, double *J, double 
  * empty classes).  Synchronizes.  Measurement variant of jqc_jk. */
 int jqc_jk_timed(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode,
                  double mixed_tau, double dens_tau, void *stream, double *class_ms);
+
+/* CUDA graph capture of any sequence of the stream-ordered calls above
+ * (jqc_jk, jqc_jk_noalloc, jqc_grad2e, jqc_grad1e, jqc_one_electron):
+ * jqc_graph_begin starts capturing `stream` (a created stream, not the
+ * legacy default stream), the calls record their kernels instead of running
+ * them, and jqc_graph_end instantiates the graph and returns its id.
+ * jqc_graph_launch replays it on a stream with the pointers and settings of
+ * the capture (write new densities into the same buffers).  Work lists and
+ * scratch must exist before the capture (one ordinary call with the same
+ * settings; otherwise the captured call fails with JQC_ERR_NOT_READY).  A
+ * new basis, pair list, partition or tuning, or an evicted work list,
+ * destroys the context's graphs; their ids then fail with JQC_ERR_INVALID.
+ * No reference counterpart (the reference runs the SCF loop eagerly in
+ * Python, scf/rhf.py:95-169). */
+int jqc_graph_begin(jqc_ctx *ctx, void *stream);
+int jqc_graph_end(jqc_ctx *ctx, void *stream, int *graph_id);
+int jqc_graph_launch(jqc_ctx *ctx, int graph_id, void *stream);
+int jqc_graph_destroy(jqc_ctx *ctx, int graph_id);
+
+/* Launch shape of each of the 21 quartet classes, cfg[3q..3q+2] = threads
+ * per block (64/128/256), lane_prims (at most that many primitive quartets
+ * per lane and task: the bra primitive pairs of a quartet are split into
+ * chunks accordingly) and persistent (1: grid capped at the resident blocks,
+ * warps stride over the task list).  Warp-engine classes use only
+ * lane_prims.  Setting a new lane_prims rebuilds the work lists.  No
+ * reference counterpart. */
+int jqc_get_tuning(jqc_ctx *ctx, int *cfg63);
+int jqc_set_tuning(jqc_ctx *ctx, const int *cfg63);
+
+/* Autotuner: times every class of the J/K build for this density, precision
+ * and screening (classes serialised, CUDA events, best of two) over threads
+ * x persistent, then over lane_prims, keeps the fastest shape per class and
+ * rebuilds the work list with it.  With cache_path, a line
+ * "signature<TAB>63 integers" is appended; a later call whose signature
+ * (device, settings, order of magnitude of each class's quartet count)
+ * matches a line applies it without timing and sets *from_cache = 1.
+ * J and K are overwritten.  Synchronizes.  No reference counterpart. */
+int jqc_autotune(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode,
+                 double mixed_tau, double dens_tau, const char *cache_path, int *from_cache, void *stream);
 
 /* FMA throughput microbenchmark on the current device: `blocks` blocks of
  * 256 threads, each 8 independent FMA chains of 16*iters steps, FP64 or

@@ -69,6 +69,15 @@ SIGNATURES = {
     "jqc_jk_timed": (_c_int, [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_dbl, _c_dbl, _vp, _dp]),
     "jqc_class_stats": (_c_int, [_vp, _c_int, _c_dbl, _llp]),
     "jqc_fp_peak": (_c_int, [_c_int, _c_int, _c_int, _dp, _vp]),
+    "jqc_batch_partition": (_c_int, [_vp, _c_int, _ip]),
+    "jqc_graph_begin": (_c_int, [_vp, _vp]),
+    "jqc_graph_end": (_c_int, [_vp, _vp, ctypes.POINTER(_c_int)]),
+    "jqc_graph_launch": (_c_int, [_vp, _c_int, _vp]),
+    "jqc_graph_destroy": (_c_int, [_vp, _c_int]),
+    "jqc_get_tuning": (_c_int, [_vp, _ip]),
+    "jqc_set_tuning": (_c_int, [_vp, _ip]),
+    "jqc_autotune": (_c_int, [_vp, _c_int, _vp, _vp, _vp, _c_int, _c_dbl, _c_dbl, ctypes.c_char_p,
+                              ctypes.POINTER(_c_int), _vp]),
 }
 
 _LIB = None

@@ -1,0 +1,534 @@
+"""Batched SCF energies, gradients and geometry optimisation for many
+molecules of uneven size on one device.
+
+The reference evaluates one geometry at a time: ``geomopt/optimizer.py:55-76``
+(``_energy_and_gradient``) rebuilds the basis, integrals, SCF and gradient for
+every call, and a sweep over geometries is a Python loop of such calls.  Here
+a whole set of molecules (different sizes, different geometries) shares one
+libjqc context.  ``jqc_batch_partition`` keeps shell pairs and quartets inside
+each molecule, so the class-sorted work list of one J/K build covers every
+molecule of the batch, and the build is one launch sequence, captured once
+into a CUDA graph and replayed in every SCF iteration.  Matrices of a batch
+are block-diagonal: molecule m owns rows and columns [off_m, off_m + n_m).
+
+* :class:`MoleculeBatch`   -- the concatenated basis and nuclei, block offsets.
+* :class:`BatchedERI`      -- the engine of a batch: J/K into fixed buffers,
+  CUDA-graph capture and replay, autotuning, gradients.
+* :func:`run_rhf_batch`    -- RHF of every molecule in lock step (per molecule
+  exactly ``scf/rhf.py:95-169``: core guess, Loewdin X, DIIS, the same
+  convergence test); a converged molecule leaves the loop and its density
+  block is zeroed, so density screening skips all of its quartets.
+* :func:`rhf_gradient_batch` -- analytic gradients of all molecules with one
+  ``jqc_grad2e`` and one ``jqc_grad1e`` call.
+* :func:`optimize_bfgs_batch` -- the BFGS of ``geomopt/optimizer.py:79-209``
+  for every molecule, each round of energy + gradient evaluations batched.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from typing import List, NamedTuple, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _abi
+from .basis import build_basis_set, build_shell_indices
+from .core import BasisSet, CalcConfig, SCFResult, SCFState, Shell, make_molecule
+from .engine import DirectERI, _ptr, _stream
+from .grad import energy_weighted_density, grad_one_electron, grad_two_electron, nuclear_repulsion_gradient
+from .integrals import nuclear_repulsion_energy
+from .scf import DIIS, diis_error, symmetric_orthogonalization
+
+# Density-screening threshold of the batched FP64 builds.  A quartet is
+# skipped only when Q_ab Q_cd max|D| < 1e-30, i.e. when its density blocks are
+# zero (the blocks of converged molecules) or its contribution is below
+# 1e-30 Eh: the builds stay FP64-exact for every active molecule.
+BATCH_DENS_TAU = 1e-30
+
+
+class _Nuclei:
+    """Nuclei of a batch in the form DirectERI reads (coords, charges)."""
+
+    def __init__(self, coords, atomic_numbers):
+        self.coords = coords
+        self.atomic_numbers = atomic_numbers
+
+
+class MoleculeBatch:
+    """Molecules of uneven size concatenated into one basis and one set of
+    nuclei, with the offsets of every molecule's atoms and basis functions.
+
+    Args:
+        mols: the molecules (Molecule records, coordinates in bohr).
+        basis: basis name used to build every molecule's basis (ignored when
+            ``bases`` is given).
+        bases: optional per-molecule BasisSet list.
+        spherical: layout of the built bases (all bases must agree).
+    """
+
+    def __init__(self, mols: Sequence, basis: str = "syn-6-31g*", bases: Optional[Sequence] = None,
+                 spherical: bool = False):
+        self.mols = list(mols)
+        if not self.mols:
+            raise ValueError("a batch needs at least one molecule")
+        if bases is None:
+            bases = [build_basis_set(m, basis, spherical=spherical) for m in self.mols]
+        if len(bases) != len(self.mols):
+            raise ValueError("one basis per molecule is required")
+        sph = {bool(getattr(b, "spherical", False)) for b in bases}
+        if len(sph) != 1:
+            raise ValueError("all bases of a batch must share the spherical/Cartesian layout")
+        self.spherical = sph.pop()
+        self.bases = list(bases)
+        shells, coords, Z, mol_of_atom = [], [], [], []
+        self.atom_off, self.n_atoms, self.bf_off, self.n_bf = [], [], [], []
+        a0 = b0 = 0
+        for m, (mol, bs) in enumerate(zip(self.mols, self.bases)):
+            na = len(np.asarray(mol.atomic_numbers))
+            for sh in bs.shells:
+                shells.append(Shell(angular_momentum=int(sh.angular_momentum),
+                                    exponents=np.asarray(sh.exponents, np.float64),
+                                    coefficients=np.asarray(sh.coefficients, np.float64),
+                                    center=np.asarray(sh.center, np.float64),
+                                    atom_index=int(sh.atom_index) + a0))
+            coords.append(np.asarray(mol.coords, np.float64))
+            Z.append(np.asarray(mol.atomic_numbers))
+            mol_of_atom += [m] * na
+            self.atom_off.append(a0)
+            self.n_atoms.append(na)
+            self.bf_off.append(b0)
+            self.n_bf.append(int(bs.n_basis))
+            a0 += na
+            b0 += int(bs.n_basis)
+        s2b, b2a, n = build_shell_indices(shells, spherical=self.spherical)
+        self.basis = BasisSet(shells=tuple(shells), n_basis=n, shell_to_basis=s2b, basis_to_atom=b2a,
+                              name="batch", spherical=self.spherical)
+        self.coords = np.concatenate(coords, axis=0)
+        self.atomic_numbers = np.concatenate(Z)
+        self.mol_of_atom = np.asarray(mol_of_atom, dtype=np.int32)
+        self.n_basis = n
+
+    def __len__(self) -> int:
+        return len(self.mols)
+
+    def nuclei(self) -> _Nuclei:
+        return _Nuclei(self.coords, self.atomic_numbers)
+
+    def block(self, M: torch.Tensor, m: int) -> torch.Tensor:
+        """View of molecule m's block of a batch matrix (last two dims)."""
+        o, k = self.bf_off[m], self.n_bf[m]
+        return M[..., o:o + k, o:o + k]
+
+    def atoms(self, g: torch.Tensor, m: int) -> torch.Tensor:
+        """Rows of molecule m in a per-atom batch array."""
+        o = self.atom_off[m]
+        return g[o:o + self.n_atoms[m]]
+
+
+class BatchedERI:
+    """Two-electron engine of a :class:`MoleculeBatch` (one libjqc context).
+
+    J/K builds write into fixed buffers so that a build can be captured into
+    a CUDA graph (``jqc_graph_begin``/``jqc_graph_end``) and replayed.
+    """
+
+    def __init__(self, batch: MoleculeBatch, device=None, schwarz_tau: float = 1e-12, prim_tau: float = 1e-20):
+        self.batch = batch
+        self.engine = DirectERI(batch.basis, batch.nuclei(), device=device, schwarz_tau=schwarz_tau,
+                                prim_tau=prim_tau, mol_of_atom=batch.mol_of_atom)
+        self.device = self.engine.device
+        self.cartesian = self.engine._C is None
+        self._capture_stream = None
+        self._graphs: List[int] = []
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self) -> None:
+        self.engine.close()
+
+    @property
+    def n_basis(self) -> int:
+        return self.engine.n_basis
+
+    @property
+    def n_cart(self) -> int:
+        return self.engine.packed.n_cart
+
+    def buffers(self, n_dens: int = 1):
+        """Zeroed (D, J, K) stacks of the batch's Cartesian size."""
+        nc = self.n_cart
+        D = torch.zeros((n_dens, nc, nc), dtype=torch.float64, device=self.device)
+        return D, torch.zeros_like(D), torch.zeros_like(D)
+
+    # ------------------------------------------------------------------ J/K
+    def jk_into(self, D, J, K, precision: str = "fp64", mixed_tau: float = 1e-7, dens_tau: float = 0.0,
+                stream=None) -> None:
+        """J/K of the stack D (Cartesian layout) into J, K (``jqc_jk``)."""
+        for t in (D, J, K):
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.shape == D.shape):
+                raise ValueError("D, J, K must be contiguous float64 CUDA tensors of one shape")
+        s = _stream(self.device) if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        with torch.cuda.device(self.device):
+            _abi.call("jqc_jk", self.engine._ctx, D.shape[0], _ptr(D), _ptr(J), _ptr(K), _abi.PREC[precision],
+                      float(mixed_tau), float(dens_tau), s)
+
+    def capture_jk(self, D, J, K, precision: str = "fp64", mixed_tau: float = 1e-7,
+                   dens_tau: float = BATCH_DENS_TAU) -> int:
+        """Capture one J/K build of the buffers D -> J, K into a CUDA graph and
+        return its id; replay with :meth:`launch`.  Runs one ordinary build
+        first (it builds the work list and the screening scratch)."""
+        if self._capture_stream is None:
+            self._capture_stream = torch.cuda.Stream(self.device)
+        s = self._capture_stream
+        cur = torch.cuda.current_stream(self.device)
+        s.wait_stream(cur)
+        sp = ctypes.c_void_p(s.cuda_stream)
+        lib = self.engine.lib
+        with torch.cuda.device(self.device):
+            self.jk_into(D, J, K, precision, mixed_tau, dens_tau, stream=s)
+            _abi.call("jqc_graph_begin", self.engine._ctx, sp)
+            gid = ctypes.c_int(-1)
+            try:
+                self.jk_into(D, J, K, precision, mixed_tau, dens_tau, stream=s)
+            except Exception:
+                if lib.jqc_graph_end(self.engine._ctx, sp, ctypes.byref(gid)) == 0:
+                    lib.jqc_graph_destroy(self.engine._ctx, gid.value)
+                raise
+            _abi.call("jqc_graph_end", self.engine._ctx, sp, ctypes.byref(gid))
+        cur.wait_stream(s)
+        self._graphs.append(gid.value)
+        return gid.value
+
+    def launch(self, graph_id: int) -> None:
+        """Replay a captured graph on the current stream."""
+        with torch.cuda.device(self.device):
+            _abi.call("jqc_graph_launch", self.engine._ctx, int(graph_id), _stream(self.device))
+
+    def autotune(self, D, J, K, precision: str = "fp64", mixed_tau: float = 1e-7,
+                 dens_tau: float = BATCH_DENS_TAU, cache_path: Optional[str] = None) -> bool:
+        """Pick the launch shape of every quartet class for this workload
+        (``jqc_autotune``); returns True when it came from the cache file."""
+        hit = ctypes.c_int(0)
+        path = cache_path.encode() if cache_path else None
+        with torch.cuda.device(self.device):
+            _abi.call("jqc_autotune", self.engine._ctx, D.shape[0], _ptr(D), _ptr(J), _ptr(K),
+                      _abi.PREC[precision], float(mixed_tau), float(dens_tau), path, ctypes.byref(hit),
+                      _stream(self.device))
+        return bool(hit.value)
+
+    def tuning(self) -> np.ndarray:
+        """(21, 3) array of (threads, lane_prims, persistent) per quartet class."""
+        out = np.zeros(63, dtype=np.int32)
+        _abi.call("jqc_get_tuning", self.engine._ctx, out.ctypes.data_as(_abi._ip))
+        return out.reshape(21, 3)
+
+    def set_tuning(self, cfg) -> None:
+        arr = np.ascontiguousarray(np.asarray(cfg, dtype=np.int32).reshape(63))
+        _abi.call("jqc_set_tuning", self.engine._ctx, arr.ctypes.data_as(_abi._ip))
+
+
+# ---------------------------------------------------------------------------
+# lock-step RHF
+# ---------------------------------------------------------------------------
+
+def _diag_groups(F_list, X_list, idx):
+    """eps, C of X^T F X for the molecules idx, one batched eigh per size."""
+    out = {}
+    by_n = {}
+    for m in idx:
+        by_n.setdefault(X_list[m].shape[0], []).append(m)
+    for _, ms in by_n.items():
+        X = torch.stack([X_list[m] for m in ms])
+        F = torch.stack([F_list[m] for m in ms])
+        e, V = torch.linalg.eigh(X.transpose(1, 2) @ F @ X)
+        C = X @ V
+        for i, m in enumerate(ms):
+            out[m] = (e[i], C[i])
+    return out
+
+
+class BatchSCF(NamedTuple):
+    """Per-molecule SCF results of a batch and the batch's build record."""
+
+    results: List[SCFResult]
+    engine: BatchedERI
+    record: dict
+
+
+def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, engine: Optional[BatchedERI] = None,
+                  use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None) -> BatchSCF:
+    """Closed-shell SCF of every molecule of the batch, in lock step.
+
+    Per molecule the iteration is that of ``scf/rhf.py:95-169`` (and of
+    :func:`jax_examples_b200.scf.run_rhf`): core-Hamiltonian guess, Loewdin
+    X = S^-1/2, F0 from the guess density, DIIS, converged when
+    dE < scf_conv and max|DIIS error| < max(scf_conv, 1e-6).  All molecules
+    share each Fock build (one graph replay of the batch J/K); a converged
+    molecule keeps its state and its density block is zeroed for the
+    remaining builds.
+    """
+    config = config or CalcConfig()
+    for mol in batch.mols:
+        if mol.spin != 0 or mol.n_electrons % 2 != 0:
+            raise ValueError("run_rhf_batch requires closed-shell molecules (spin 0, even electron count)")
+    eng = engine or BatchedERI(batch, schwarz_tau=config.schwarz_tau)
+    dev = eng.device
+    M = len(batch)
+    t_setup = time.perf_counter()
+    S_all, T_all, V_all = eng.engine.one_electron()
+    H_all = T_all + V_all
+    S = [batch.block(S_all, m).clone() for m in range(M)]
+    H = [batch.block(H_all, m).clone() for m in range(M)]
+    X = [symmetric_orthogonalization(s) for s in S]
+    n_occ = [mol.n_electrons // 2 for mol in batch.mols]
+    E_nuc = [nuclear_repulsion_energy(mol) for mol in batch.mols]
+
+    Dbuf, Jbuf, Kbuf = eng.buffers(1)
+    cart = eng.cartesian
+    graph = None
+    events = []
+
+    def fock(dens: dict) -> dict:
+        """F_m = H_m + J_m - K_m / 2 for the molecules in dens (others zeroed)."""
+        if cart:
+            Dbuf.zero_()
+            for m, d in dens.items():
+                batch.block(Dbuf[0], m).copy_(d)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if graph is not None:
+                eng.launch(graph)
+            else:
+                eng.jk_into(Dbuf, Jbuf, Kbuf, "fp64", dens_tau=BATCH_DENS_TAU)
+            e1.record()
+            events.append((e0, e1))
+            J, K = Jbuf[0], Kbuf[0]
+        else:
+            Dfull = torch.zeros((eng.n_basis, eng.n_basis), dtype=torch.float64, device=dev)
+            for m, d in dens.items():
+                batch.block(Dfull, m).copy_(d)
+            J, K = eng.engine.jk(Dfull, dens_tau=BATCH_DENS_TAU)
+        return {m: H[m] + batch.block(J, m) - 0.5 * batch.block(K, m) for m in dens}
+
+    # core guess (rhf.py:111-121)
+    all_m = list(range(M))
+    dg = _diag_groups(H, X, all_m)
+    D = {m: 2.0 * dg[m][1][:, :n_occ[m]] @ dg[m][1][:, :n_occ[m]].T for m in all_m}
+    if cart and (use_graph or autotune):
+        for m in all_m:
+            batch.block(Dbuf[0], m).copy_(D[m])
+        if autotune:
+            eng.autotune(Dbuf, Jbuf, Kbuf, "fp64", dens_tau=BATCH_DENS_TAU, cache_path=tune_cache)
+        if use_graph:
+            graph = eng.capture_jk(Dbuf, Jbuf, Kbuf, "fp64", dens_tau=BATCH_DENS_TAU)
+    setup_s = time.perf_counter() - t_setup
+    F = fock(D)
+    dg = _diag_groups(F, X, all_m)
+    eps = {m: dg[m][0] for m in all_m}
+    C = {m: dg[m][1] for m in all_m}
+    E = torch.stack([0.5 * torch.sum(D[m] * (H[m] + F[m])) for m in all_m]).cpu().numpy()
+    last = E.copy()
+    diis = [DIIS(config.diis_space) for _ in all_m]
+    iters = [0] * M
+    converged = [False] * M
+    active = list(all_m)
+    n_builds = 1
+    for _ in range(config.max_scf_iter):
+        if not active:
+            break
+        Fn = fock({m: D[m] for m in active})
+        n_builds += 1
+        if config.damping > 0.0:
+            Fn = {m: (1.0 - config.damping) * Fn[m] + config.damping * F[m] for m in active}
+        err = {m: diis_error(Fn[m], D[m], S[m], X[m]) for m in active}
+        Fx = {m: diis[m].extrapolate(Fn[m], err[m]) for m in active}
+        dg = _diag_groups(Fx, X, active)
+        for m in active:
+            eps[m], C[m] = dg[m]
+            D[m] = 2.0 * C[m][:, :n_occ[m]] @ C[m][:, :n_occ[m]].T
+            F[m] = Fx[m]
+            iters[m] += 1
+        En = torch.stack([0.5 * torch.sum(D[m] * (H[m] + Fx[m])) for m in active]).cpu().numpy()
+        emax = torch.stack([torch.max(torch.abs(err[m])) for m in active]).cpu().numpy()
+        still = []
+        for i, m in enumerate(active):
+            E[m] = En[i]
+            dE = abs(E[m] - last[m])
+            last[m] = E[m]
+            if dE < config.scf_conv and emax[i] < max(config.scf_conv, 1e-6):
+                converged[m] = True
+            else:
+                still.append(m)
+        active = still
+    jk_s = 0.0
+    if events:
+        events[-1][1].synchronize()
+        jk_s = sum(a.elapsed_time(b) for a, b in events) * 1e-3
+    record = {"fock_builds": n_builds, "jk_seconds": jk_s, "setup_seconds": setup_s, "graph": graph is not None,
+              "autotuned": bool(autotune), "n_molecules": M, "n_basis": batch.n_basis}
+    results = []
+    for m in all_m:
+        st = SCFState(density=D[m], fock=F[m], coefficients=C[m], orbital_energies=eps[m], energy=float(E[m]),
+                      iteration=iters[m])
+        results.append(SCFResult(converged=converged[m], state=st, energy=float(E[m]) + E_nuc[m],
+                                 E_elec=float(E[m]), E_nuc=E_nuc[m], n_iterations=iters[m], S=S[m], H_core=H[m],
+                                 ERI=None, precision={"precision": "fp64", "batched": True}))
+    return BatchSCF(results=results, engine=eng, record=record)
+
+
+def rhf_gradient_batch(batch: MoleculeBatch, scf: BatchSCF, timing: Optional[dict] = None) -> List[torch.Tensor]:
+    """Analytic RHF gradients (n_atoms_m, 3) of every molecule of the batch:
+    one ``jqc_grad2e`` and one ``jqc_grad1e`` call over the block-diagonal
+    densities (the per-molecule expression of
+    :func:`jax_examples_b200.grad.rhf_gradient`)."""
+    eng = scf.engine
+    dev = eng.device
+    n = eng.n_basis
+    D = torch.zeros((n, n), dtype=torch.float64, device=dev)
+    W = torch.zeros_like(D)
+    for m, res in enumerate(scf.results):
+        st = res.state
+        batch.block(D, m).copy_(st.density)
+        batch.block(W, m).copy_(energy_weighted_density(st.coefficients, st.orbital_energies,
+                                                        batch.mols[m].n_electrons // 2))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    g = grad_one_electron(eng.engine, D, W) + grad_two_electron(eng.engine, [D], 1.0, 0.5)
+    e1.record()
+    e1.synchronize()
+    if timing is not None:
+        timing["grad_seconds"] = timing.get("grad_seconds", 0.0) + e0.elapsed_time(e1) * 1e-3
+    out = []
+    for m, mol in enumerate(batch.mols):
+        gn = nuclear_repulsion_gradient(mol.coords, mol.atomic_numbers).to(dev)
+        out.append(batch.atoms(g, m) + gn)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# batched BFGS
+# ---------------------------------------------------------------------------
+
+class OptResult(NamedTuple):
+    """Result of a geometry optimisation (``geomopt/optimizer.py:36-52``)."""
+
+    converged: bool
+    molecule: object
+    energy: float
+    gradient: np.ndarray
+    n_steps: int
+    trajectory: list
+
+
+def _bfgs_walker(mol, max_steps: int, grad_tol: float, step_tol: float, max_step_size: float):
+    """BFGS of ``geomopt/optimizer.py:79-209`` for one molecule, written as a
+    generator: it yields the coordinates it needs evaluated and receives
+    (energy, gradient) back, so many walkers can share batched evaluations.
+    Identity initial inverse Hessian, step clipped to max_step_size, Armijo
+    backtracking (c1 = 1e-4, at most 10 halvings, the last trial accepted
+    when none passes), BFGS update when s.y > 1e-10."""
+    coords = np.asarray(mol.coords, dtype=np.float64).copy()
+    n_atoms = coords.shape[0]
+    n_dof = 3 * n_atoms
+    energy, grad = yield coords
+    g = np.asarray(grad, dtype=np.float64).reshape(-1)
+    H_inv = np.eye(n_dof)
+    trajectory = [(coords.copy(), energy)]
+    converged = False
+    for _step in range(1, max_steps + 1):
+        g_max = float(np.max(np.abs(g)))
+        if g_max < grad_tol:
+            converged = True
+            break
+        direction = -H_inv @ g
+        norm = float(np.linalg.norm(direction))
+        if norm > max_step_size:
+            direction = direction * (max_step_size / norm)
+        alpha, c1 = 1.0, 1e-4
+        e_old, g_old = energy, g.copy()
+        for _ in range(10):
+            new_coords = coords + alpha * direction.reshape(n_atoms, 3)
+            e_new, g_new = yield new_coords
+            if e_new <= e_old + c1 * alpha * float(np.dot(g_old, direction)):
+                break
+            alpha *= 0.5
+        s = (alpha * direction).reshape(-1)
+        coords = new_coords
+        energy = e_new
+        g_new = np.asarray(g_new, dtype=np.float64).reshape(-1)
+        y = g_new - g_old
+        s_max = float(np.max(np.abs(s)))
+        if s_max < step_tol and g_max < grad_tol * 10:
+            converged = True
+            g = g_new
+            trajectory.append((coords.copy(), energy))
+            break
+        sy = float(np.dot(s, y))
+        if sy > 1e-10:
+            rho = 1.0 / sy
+            V = np.eye(n_dof) - rho * np.outer(s, y)
+            H_inv = V @ H_inv @ V.T + rho * np.outer(s, s)
+        g = g_new
+        trajectory.append((coords.copy(), energy))
+    final = make_molecule(mol.elements, coords, np.asarray(mol.atomic_numbers), charge=mol.charge, spin=mol.spin)
+    return OptResult(converged=converged, molecule=final, energy=energy, gradient=g.reshape(n_atoms, 3),
+                     n_steps=len(trajectory) - 1, trajectory=trajectory)
+
+
+def energies_and_gradients(mols: Sequence, basis: str = "syn-6-31g*", config: Optional[CalcConfig] = None,
+                           use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None,
+                           timing: Optional[dict] = None):
+    """RHF energies and analytic gradients of many molecules in one batch:
+    ``[(energy, gradient (n_atoms, 3) ndarray, SCFResult)]``."""
+    batch = MoleculeBatch(mols, basis)
+    scf = run_rhf_batch(batch, config, use_graph=use_graph, autotune=autotune, tune_cache=tune_cache)
+    grads = rhf_gradient_batch(batch, scf, timing)
+    if timing is not None:
+        timing["jk_seconds"] = timing.get("jk_seconds", 0.0) + scf.record["jk_seconds"]
+        timing["fock_builds"] = timing.get("fock_builds", 0) + scf.record["fock_builds"]
+        timing["evaluations"] = timing.get("evaluations", 0) + len(mols)
+        timing["batches"] = timing.get("batches", 0) + 1
+    out = [(r.energy, g.cpu().numpy(), r) for r, g in zip(scf.results, grads)]
+    scf.engine.close()
+    return out
+
+
+def optimize_bfgs_batch(mols: Sequence, basis: str = "syn-6-31g*", max_steps: int = 50, grad_tol: float = 1e-4,
+                        step_tol: float = 1e-6, scf_conv: float = 1e-10, max_step_size: float = 0.3,
+                        config: Optional[CalcConfig] = None, use_graph: bool = True, autotune: bool = False,
+                        tune_cache: Optional[str] = None, timing: Optional[dict] = None) -> List[OptResult]:
+    """BFGS geometry optimisation of every molecule (``optimize_bfgs`` of
+    ``geomopt/optimizer.py:79-209`` per molecule, RHF).  Every round collects
+    the geometry each unfinished optimisation needs next (a step or a
+    line-search trial) and evaluates all of them in one batch."""
+    config = config or CalcConfig(scf_conv=scf_conv, max_scf_iter=200)
+    walkers = [_bfgs_walker(m, max_steps, grad_tol, step_tol, max_step_size) for m in mols]
+    pending = {i: w.send(None) for i, w in enumerate(walkers)}
+    results: List[Optional[OptResult]] = [None] * len(mols)
+    while pending:
+        ids = sorted(pending)
+        geoms = [make_molecule(mols[i].elements, pending[i], np.asarray(mols[i].atomic_numbers),
+                               charge=mols[i].charge, spin=mols[i].spin) for i in ids]
+        evals = energies_and_gradients(geoms, basis, config, use_graph=use_graph, autotune=autotune,
+                                       tune_cache=tune_cache, timing=timing)
+        nxt = {}
+        for i, (e, g, _res) in zip(ids, evals):
+            try:
+                nxt[i] = walkers[i].send((e, g))
+            except StopIteration as stop:
+                results[i] = stop.value
+        pending = nxt
+    return results
+
+
+def optimize_bfgs(mol, basis_name: str = "syn-6-31g*", method: str = "rhf", max_steps: int = 50,
+                  grad_tol: float = 1e-4, step_tol: float = 1e-6, scf_conv: float = 1e-10,
+                  max_step_size: float = 0.3, verbose: int = 0) -> OptResult:
+    """Single-molecule ``optimize_bfgs`` (``geomopt/optimizer.py:79-209``)
+    with the device SCF and the analytic gradient."""
+    if method != "rhf":
+        raise NotImplementedError("optimize_bfgs: only method='rhf' is implemented on the batched path")
+    return optimize_bfgs_batch([mol], basis_name, max_steps, grad_tol, step_tol, scf_conv, max_step_size)[0]

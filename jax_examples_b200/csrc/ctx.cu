@@ -2,6 +2,8 @@
 // Schwarz bounds, class-sorted work lists and the extern "C" entry points.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -35,6 +37,8 @@ struct OneEParams {
   const int* ao;
   const double* atom_xyz;
   const double* atom_Z;
+  const int* shell_mol;  // molecule of each shell / atom (nullptr: one molecule)
+  const int* atom_mol;
   const double* boys;
   double* S;
   double* T;
@@ -172,12 +176,22 @@ struct TaskSet {
   long long class_prims[2][kNumQuartetClasses] = {};
 };
 
+// Pairs of one (class, primitive-pair count, molecule), Q descending.
 struct Block {
-  int pc, ka, kb, start, count;
+  int pc, ka, kb, start, count, mol;
 };
 
-// Upper bound on primitive quartets one lane evaluates per task.
+// Upper bound on primitive quartets one lane evaluates per task (default).
 constexpr int kMaxLanePrims = 256;
+
+// Launch shape of one quartet class, picked by the autotuner: threads per
+// block, the bra primitive-pair chunk (at most lane_prims primitive quartets
+// per lane and task) and whether the grid is capped at the resident blocks.
+struct ClassTune {
+  int threads = 128;
+  int lane_prims = kMaxLanePrims;
+  int persistent = 0;
+};
 constexpr int kNumStreams = 4;
 
 }  // namespace jqc
@@ -194,6 +208,10 @@ struct jqc_ctx {
   DevBuf<int> d_ao, d_l, d_atom, d_nprim, d_prim_off;
   DevBuf<double> d_atom_xyz, d_atom_Z, d_exps, d_coefs;
   bool basis_ready = false;
+  // batch partition: molecule of each shell / atom (one molecule by default)
+  int n_mol = 1;
+  std::vector<int> shell_mol, atom_mol;
+  DevBuf<int> d_shell_mol, d_atom_mol;
   // pairs (sorted: block by (class, K_a, K_b), Q descending inside)
   bool pairs_ready = false;
   double tau = 0.0;
@@ -213,11 +231,15 @@ struct jqc_ctx {
   DevBuf<float> d_dmax;
   cudaStream_t side[kNumStreams] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kNumStreams] = {};
+  cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // per-class timing
   const double* boys64 = nullptr;
   const float* boys32 = nullptr;
   const double* boysA64 = nullptr;  // aligned per-order tables (hot kernels)
   const float* boysA32 = nullptr;
   double prim_tau = 0.0;
+  ClassTune tune[kNumQuartetClasses];
+  // CUDA graphs captured through jqc_graph_begin / jqc_graph_end
+  std::vector<cudaGraphExec_t> graphs;
 };
 
 namespace jqc {
@@ -271,12 +293,17 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
   long long nq[2] = {0, 0}, npq = 0;
   long long cq[2][kNumQuartetClasses] = {}, cp[2][kNumQuartetClasses] = {};
   const double tau = full ? 0.0 : c->tau;
+  // Quartets pair a bra and a ket of the same molecule: ket blocks by molecule.
+  std::vector<std::vector<int>> mol_blocks(c->n_mol);
+  for (size_t cb = 0; cb < c->blocks.size(); ++cb) mol_blocks[c->blocks[cb].mol].push_back((int)cb);
   for (size_t cb = 0; cb < c->blocks.size(); ++cb) {
     const Block& B = c->blocks[cb];
     for (int pi = 0; pi < B.count; ++pi) {
       const int gi = B.start + pi;
       const double Qi = c->pairs[gi].Q;
-      for (size_t ck = 0; ck <= cb; ++ck) {
+      for (const int ckb : mol_blocks[B.mol]) {
+        const size_t ck = (size_t)ckb;
+        if (ck > cb) break;
         const Block& K = c->blocks[ck];
         const int limit = (ck == cb) ? pi + 1 : K.count;
         const int n_all = prefix_count(c->pairs, K.start, limit, Qi, tau);
@@ -285,11 +312,11 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
         if (mode == JQC_PREC_MIXED) n64 = std::min(n_all, prefix_count(c->pairs, K.start, limit, Qi, mixed_tau));
         const int qc = quartet_class(B.pc, K.pc);
         const int seg[3] = {0, n64, n_all};
-        // Split the bra primitive pairs so one lane does at most ~kMaxLanePrims
+        // Split the bra primitive pairs so one lane does at most ~lane_prims
         // primitive quartets per task (the tensor keeps whole quartets).
         const int nbp = c->pairs[gi].npp, nkp = K.ka * K.kb;
         int chunk = nbp;
-        if (!full && !grad) chunk = std::max(1, std::min(nbp, kMaxLanePrims / std::max(1, nkp)));
+        if (!full && !grad) chunk = std::max(1, std::min(nbp, c->tune[qc].lane_prims / std::max(1, nkp)));
         // Register classes: 32 kets per warp task (one per lane).  Warp-engine
         // classes: one ket per task, so every quartet gets its own warp.
         const int per_task = grad ? (is_grad_reg_class(qc) ? 32 : 1) : (is_reg_class(qc) ? 32 : 1);
@@ -348,6 +375,8 @@ static int ensure_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, boo
   return build_tasks(c, ts, mode, mixed_tau, full, s);
 }
 
+static void drop_graphs(jqc_ctx* c);
+
 // J/K work list for (mode, mixed_tau), built once and kept (a few per context).
 static int ensure_jk_tasks(jqc_ctx* c, int mode, double mixed_tau, cudaStream_t s) {
   if (mode != JQC_PREC_MIXED) mixed_tau = 0.0;
@@ -357,6 +386,7 @@ static int ensure_jk_tasks(jqc_ctx* c, int mode, double mixed_tau, cudaStream_t 
       return JQC_OK;
     }
   if (c->jk_cache.size() >= 4) {
+    drop_graphs(c);
     delete c->jk_cache.front();
     c->jk_cache.erase(c->jk_cache.begin());
   }
@@ -371,7 +401,18 @@ static int ensure_jk_tasks(jqc_ctx* c, int mode, double mixed_tau, cudaStream_t 
   return JQC_OK;
 }
 
+// Captured graphs hold pointers to the work lists and pair data: whatever
+// frees or replaces those destroys the graphs first (their ids then fail).
+static void drop_graphs(jqc_ctx* c) {
+  for (cudaGraphExec_t& g : c->graphs)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
 static void drop_jk_tasks(jqc_ctx* c) {
+  drop_graphs(c);
   for (TaskSet* ts : c->jk_cache) delete ts;
   c->jk_cache.clear();
   c->jk_cur = nullptr;
@@ -379,6 +420,87 @@ static void drop_jk_tasks(jqc_ctx* c) {
 
 static int select_device(const jqc_ctx* c) {
   JQC_CUDA_CHECK(cudaSetDevice(c->device));
+  return JQC_OK;
+}
+
+static bool stream_capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) return false;
+  return st == cudaStreamCaptureStatusActive;
+}
+
+static TaskSet* find_jk_tasks(jqc_ctx* c, int mode, double mixed_tau) {
+  if (mode != JQC_PREC_MIXED) mixed_tau = 0.0;
+  for (TaskSet* ts : c->jk_cache)
+    if (ts->valid && ts->mode == mode && ts->mixed_tau == mixed_tau) return ts;
+  return nullptr;
+}
+
+// One J/K build over work list `ts`: zero J/K, density maxima (when dmax is
+// given), the class kernels on the side streams (forked from and joined back
+// into s; they only add into J/K with atomics), then J = A + A^T, K = B + B^T.
+// With class_ms the classes run one after another on s, each timed.  Only
+// stream operations: no allocation, no host synchronisation except for the
+// timed form, so the untimed form can be captured into a CUDA graph.
+static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D, double* J, double* K,
+                      float* dmax, double dens_tau, cudaStream_t s, double* class_ms) {
+  const int n = c->n_bf;
+  const size_t nn = (size_t)n * n * n_dens;
+  JQC_CUDA_CHECK(cudaMemsetAsync(J, 0, nn * sizeof(double), s));
+  JQC_CUDA_CHECK(cudaMemsetAsync(K, 0, nn * sizeof(double), s));
+  if (class_ms)
+    for (int k = 0; k < 2 * kNumQuartetClasses; ++k) class_ms[k] = 0.0;
+  if (dens_tau > 0.0 && dmax != nullptr)
+    JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, dmax, s));
+  else
+    dmax = nullptr;
+  if (!class_ms) {
+    JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
+    for (int i = 0; i < kNumStreams; ++i) JQC_CUDA_CHECK(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
+  }
+  int li = 0;
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      JKParams p;
+      p.tasks = ts->d.ptr + ts->off[prec][qc];
+      p.n_tasks = ts->cnt[prec][qc];
+      if (p.n_tasks == 0) continue;
+      p.pairs = c->d_pairs.ptr;
+      p.pp = prec ? (const void*)c->d_ppf.ptr : (const void*)c->d_pp.ptr;
+      p.centres = c->d_centres.ptr;
+      p.ao = c->d_ao.ptr;
+      p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
+      p.boys_al = prec ? (const void*)c->boysA32 : (const void*)c->boysA64;
+      p.D = D;
+      p.J = J;
+      p.K = K;
+      p.n = n;
+      p.n_dens = n_dens;
+      p.dmax = dmax;
+      p.n_shell = c->n_shell;
+      p.dens_tau = (float)dens_tau;
+      p.threads = c->tune[qc].threads;
+      p.persistent = c->tune[qc].persistent;
+      if (class_ms) {
+        JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));
+        JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, s));
+        JQC_CUDA_CHECK(cudaEventRecord(c->ev_t1, s));
+        JQC_CUDA_CHECK(cudaEventSynchronize(c->ev_t1));
+        float ms = 0.f;
+        JQC_CUDA_CHECK(cudaEventElapsedTime(&ms, c->ev_t0, c->ev_t1));
+        class_ms[prec * kNumQuartetClasses + qc] = ms;
+      } else {
+        JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, c->side[li++ % kNumStreams]));
+      }
+    }
+  if (!class_ms) {
+    for (int i = 0; i < kNumStreams; ++i) {
+      JQC_CUDA_CHECK(cudaEventRecord(c->ev_join[i], c->side[i]));
+      JQC_CUDA_CHECK(cudaStreamWaitEvent(s, c->ev_join[i], 0));
+    }
+  }
+  JQC_CUDA_CHECK(launch_symmetrize(J, n_dens, n, s));
+  JQC_CUDA_CHECK(launch_symmetrize(K, n_dens, n, s));
   return JQC_OK;
 }
 
@@ -416,6 +538,8 @@ int jqc_ctx_create(int device, jqc_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev_t0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev_t1);
   if (e != cudaSuccess) {
     set_error(std::string("jqc_ctx_create: ") + cudaGetErrorString(e));
     jqc_ctx_destroy(c);
@@ -433,6 +557,10 @@ int jqc_ctx_destroy(jqc_ctx* ctx) {
       if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_t0) cudaEventDestroy(ctx->ev_t0);
+    if (ctx->ev_t1) cudaEventDestroy(ctx->ev_t1);
+    for (cudaGraphExec_t g : ctx->graphs)
+      if (g) cudaGraphExecDestroy(g);
     drop_jk_tasks(ctx);
     delete ctx;
   }
@@ -498,8 +626,36 @@ int jqc_basis_upload(jqc_ctx* c, int n_shell, const int* l, const int* nprim, co
     JQC_CUDA_CHECK(c->d_atom_xyz.upload(c->atom_xyz, s0));
     JQC_CUDA_CHECK(c->d_atom_Z.upload(c->atom_Z, s0));
   }
+  c->n_mol = 1;
+  c->shell_mol.assign(n_shell, 0);
+  c->atom_mol.assign(n_atom, 0);
   JQC_CUDA_CHECK(cudaStreamSynchronize(s0));
   c->basis_ready = true;
+  c->pairs_ready = false;
+  drop_jk_tasks(c);
+  c->full_tasks.valid = false;
+  c->grad_tasks.valid = false;
+  return JQC_OK;
+}
+
+int jqc_batch_partition(jqc_ctx* c, int n_mol, const int* mol_of_atom) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_batch_partition: null context");
+  JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_batch_partition: call jqc_basis_upload first");
+  JQC_REQUIRE(c->n_atom > 0, JQC_ERR_NOT_READY, "jqc_batch_partition: the basis was uploaded without atoms");
+  JQC_REQUIRE(n_mol >= 1 && n_mol <= c->n_atom, JQC_ERR_INVALID, "jqc_batch_partition: n_mol out of range");
+  JQC_REQUIRE(mol_of_atom != nullptr, JQC_ERR_INVALID, "jqc_batch_partition: null mol_of_atom");
+  for (int a = 0; a < c->n_atom; ++a)
+    JQC_REQUIRE(mol_of_atom[a] >= 0 && mol_of_atom[a] < n_mol, JQC_ERR_INVALID,
+                "jqc_batch_partition: molecule index out of range");
+  int rc = select_device(c);
+  if (rc) return rc;
+  c->n_mol = n_mol;
+  c->atom_mol.assign(mol_of_atom, mol_of_atom + c->n_atom);
+  for (int s = 0; s < c->n_shell; ++s) c->shell_mol[s] = c->atom_mol[c->atom[s]];
+  cudaStream_t s0 = 0;
+  JQC_CUDA_CHECK(c->d_shell_mol.upload(c->shell_mol, s0));
+  JQC_CUDA_CHECK(c->d_atom_mol.upload(c->atom_mol, s0));
+  JQC_CUDA_CHECK(cudaStreamSynchronize(s0));
   c->pairs_ready = false;
   drop_jk_tasks(c);
   c->full_tasks.valid = false;
@@ -523,6 +679,7 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, double prim_tau, void* strea
   std::vector<int> ids[kNumPairClasses];
   for (int i = 0; i < c->n_shell; ++i)
     for (int j = 0; j <= i; ++j) {
+      if (c->shell_mol[i] != c->shell_mol[j]) continue;  // no pairs across molecules
       int a = i, b = j;
       if (c->l[a] < c->l[b]) std::swap(a, b);
       ShellPair sp;
@@ -570,23 +727,25 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, double prim_tau, void* strea
   JQC_CUDA_CHECK(cudaMemcpyAsync(qbits.data(), d_q.ptr, qbits.size() * sizeof(unsigned long long),
                                  cudaMemcpyDeviceToHost, s));
   JQC_CUDA_CHECK(cudaStreamSynchronize(s));
-  double qmax = 0.0;
+  std::vector<double> qmax(c->n_mol, 0.0);  // largest Q of each molecule
   c->Qmat.assign((size_t)c->n_shell * c->n_shell, 0.0);
   for (size_t k = 0; k < raw.size(); ++k) {
     double v;
     std::memcpy(&v, &qbits[k], sizeof(double));
     raw[k].Q = std::sqrt(std::max(v, 0.0));
-    qmax = std::max(qmax, raw[k].Q);
+    double& qm = qmax[c->shell_mol[raw[k].a]];
+    qm = std::max(qm, raw[k].Q);
     c->Qmat[(size_t)raw[k].a * c->n_shell + raw[k].b] = raw[k].Q;
     c->Qmat[(size_t)raw[k].b * c->n_shell + raw[k].a] = raw[k].Q;
   }
-  // 3. drop pairs that cannot pass, sort by (class, K_a, K_b) then Q desc
+  // 3. drop pairs that cannot pass with any pair of their molecule, sort by
+  // (class, primitive pairs, molecule) then Q descending
   std::vector<int> keep;
   for (size_t k = 0; k < raw.size(); ++k)
-    if (raw[k].Q * qmax >= schwarz_tau && raw[k].Q > 0.0) keep.push_back((int)k);
+    if (raw[k].Q * qmax[c->shell_mol[raw[k].a]] >= schwarz_tau && raw[k].Q > 0.0) keep.push_back((int)k);
   auto key = [&](int k) {
     const ShellPair& p = raw[k];
-    return std::make_tuple(p.cls, p.npp, 1);
+    return std::make_tuple(p.cls, p.npp, c->shell_mol[p.a]);
   };
   std::stable_sort(keep.begin(), keep.end(), [&](int x, int y) {
     auto kx = key(x), ky = key(y);
@@ -609,8 +768,8 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, double prim_tau, void* strea
     }
     auto kk = key(keep[r]);
     if (c->blocks.empty() || std::get<0>(kk) != c->blocks.back().pc || std::get<1>(kk) != c->blocks.back().ka ||
-        std::get<2>(kk) != c->blocks.back().kb) {
-      c->blocks.push_back(Block{std::get<0>(kk), std::get<1>(kk), std::get<2>(kk), (int)c->pairs.size(), 0});
+        std::get<2>(kk) != c->blocks.back().mol) {
+      c->blocks.push_back(Block{std::get<0>(kk), std::get<1>(kk), 1, (int)c->pairs.size(), 0, std::get<2>(kk)});
     }
     c->blocks.back().count++;
     c->pairs.push_back(sp);
@@ -738,6 +897,7 @@ int jqc_eri_tensor(jqc_ctx* c, double* out, long long max_bytes, void* stream) {
   int rc = select_device(c);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  JQC_REQUIRE(!stream_capturing(s), JQC_ERR_INVALID, "jqc_eri_tensor: cannot run inside a graph capture");
   rc = ensure_tasks(c, c->full_tasks, JQC_PREC_FP64, 0.0, true, s);
   if (rc) return rc;
   JQC_CUDA_CHECK(cudaMemsetAsync(out, 0, (size_t)bytes, s));
@@ -767,6 +927,8 @@ int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k
   int rc = select_device(c);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  JQC_REQUIRE(c->grad_tasks.valid || !stream_capturing(s), JQC_ERR_NOT_READY,
+              "jqc_grad2e: no gradient work list; call jqc_grad2e once before the capture");
   if (!c->grad_tasks.valid) {
     rc = build_tasks(c, c->grad_tasks, JQC_PREC_FP64, 0.0, false, s, true);
     if (rc) return rc;
@@ -818,6 +980,8 @@ int jqc_grad1e(jqc_ctx* c, const double* D, const double* W, double* grad, void*
   p.atom = c->d_atom.ptr;
   p.atom_xyz = c->d_atom_xyz.ptr;
   p.atom_Z = c->d_atom_Z.ptr;
+  p.shell_mol = c->n_mol > 1 ? c->d_shell_mol.ptr : nullptr;
+  p.atom_mol = c->n_mol > 1 ? c->d_atom_mol.ptr : nullptr;
   p.boys = c->boys64;
   p.D = D;
   p.W = W;
@@ -844,6 +1008,8 @@ int jqc_one_electron(jqc_ctx* c, double* S, double* T, double* V, void* stream) 
   p.ao = c->d_ao.ptr;
   p.atom_xyz = c->d_atom_xyz.ptr;
   p.atom_Z = c->d_atom_Z.ptr;
+  p.shell_mol = c->n_mol > 1 ? c->d_shell_mol.ptr : nullptr;
+  p.atom_mol = c->n_mol > 1 ? c->d_atom_mol.ptr : nullptr;
   p.boys = c->boys64;
   p.S = S;
   p.T = T;
@@ -877,68 +1043,261 @@ static int jk_impl(jqc_ctx* c, int n_dens, const double* D, double* J, double* K
   JQC_REQUIRE(mixed_tau >= 0.0 && dens_tau >= 0.0, JQC_ERR_INVALID, "jqc_jk: thresholds must be >= 0");
   int rc = select_device(c);
   if (rc) return rc;
+  const bool capturing = stream_capturing(s);
+  JQC_REQUIRE(!(capturing && class_ms), JQC_ERR_INVALID, "jqc_jk_timed: cannot run inside a graph capture");
+  if (capturing) {
+    // inside a capture nothing may be allocated or uploaded
+    JQC_REQUIRE(find_jk_tasks(c, precision_mode, mixed_tau) != nullptr, JQC_ERR_NOT_READY,
+                "jqc_jk: no work list for this precision_mode/mixed_tau; call jqc_jk once before the capture");
+    JQC_REQUIRE(dens_tau <= 0.0 || c->d_dmax.n >= (size_t)c->n_shell * c->n_shell, JQC_ERR_NOT_READY,
+                "jqc_jk: density screening scratch not allocated; call jqc_jk once before the capture");
+  }
   rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
   if (rc) return rc;
-  const int n = c->n_bf;
-  const size_t nn = (size_t)n * n * n_dens;
-  JQC_CUDA_CHECK(cudaMemsetAsync(J, 0, nn * sizeof(double), s));
-  JQC_CUDA_CHECK(cudaMemsetAsync(K, 0, nn * sizeof(double), s));
-  if (class_ms)
-    for (int k = 0; k < 2 * kNumQuartetClasses; ++k) class_ms[k] = 0.0;
-  const float* dmax = nullptr;
+  float* dmax = nullptr;
   if (dens_tau > 0.0) {
     JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
-    JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, c->d_dmax.ptr, s));
     dmax = c->d_dmax.ptr;
   }
-  // Class kernels run concurrently on the context's side streams (they only
-  // add into J/K with atomics), forked from and joined back into `stream`.
-  JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
-  for (int i = 0; i < kNumStreams; ++i) JQC_CUDA_CHECK(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
-  int li = 0;
+  return run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dens_tau, s, class_ms);
+}
+
+// ----------------------------------------------------------- CUDA graphs
+int jqc_graph_begin(jqc_ctx* c, void* stream) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_graph_begin: null context");
+  JQC_REQUIRE(stream != nullptr, JQC_ERR_INVALID,
+              "jqc_graph_begin: the legacy default stream cannot be captured; pass a created stream");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  JQC_REQUIRE(!stream_capturing(s), JQC_ERR_INVALID, "jqc_graph_begin: the stream is already capturing");
+  JQC_CUDA_CHECK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  return JQC_OK;
+}
+
+int jqc_graph_end(jqc_ctx* c, void* stream, int* graph_id) {
+  JQC_REQUIRE(c && graph_id, JQC_ERR_INVALID, "jqc_graph_end: null argument");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaGraph_t g = nullptr;
+  JQC_CUDA_CHECK(cudaStreamEndCapture(s, &g));
+  JQC_REQUIRE(g != nullptr, JQC_ERR_CUDA, "jqc_graph_end: the capture produced no graph");
+  cudaGraphExec_t ex = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  JQC_CUDA_CHECK(e);
+  c->graphs.push_back(ex);
+  *graph_id = (int)c->graphs.size() - 1;
+  return JQC_OK;
+}
+
+int jqc_graph_launch(jqc_ctx* c, int graph_id, void* stream) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_graph_launch: null context");
+  JQC_REQUIRE(graph_id >= 0 && graph_id < (int)c->graphs.size() && c->graphs[graph_id], JQC_ERR_INVALID,
+              "jqc_graph_launch: unknown graph id, or the graph was invalidated by a new basis, pair list, "
+              "work list or tuning");
+  int rc = select_device(c);
+  if (rc) return rc;
+  JQC_CUDA_CHECK(cudaGraphLaunch(c->graphs[graph_id], static_cast<cudaStream_t>(stream)));
+  return JQC_OK;
+}
+
+int jqc_graph_destroy(jqc_ctx* c, int graph_id) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_graph_destroy: null context");
+  JQC_REQUIRE(graph_id >= 0 && graph_id < (int)c->graphs.size(), JQC_ERR_INVALID,
+              "jqc_graph_destroy: unknown graph id");
+  int rc = select_device(c);
+  if (rc) return rc;
+  if (c->graphs[graph_id]) JQC_CUDA_CHECK(cudaGraphExecDestroy(c->graphs[graph_id]));
+  c->graphs[graph_id] = nullptr;
+  return JQC_OK;
+}
+
+// ------------------------------------------------------------ autotuning
+int jqc_get_tuning(jqc_ctx* c, int* out) {
+  JQC_REQUIRE(c && out, JQC_ERR_INVALID, "jqc_get_tuning: null argument");
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    out[3 * qc] = c->tune[qc].threads;
+    out[3 * qc + 1] = c->tune[qc].lane_prims;
+    out[3 * qc + 2] = c->tune[qc].persistent;
+  }
+  return JQC_OK;
+}
+
+int jqc_set_tuning(jqc_ctx* c, const int* cfg) {
+  JQC_REQUIRE(c && cfg, JQC_ERR_INVALID, "jqc_set_tuning: null argument");
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    const int th = cfg[3 * qc], lp = cfg[3 * qc + 1], pe = cfg[3 * qc + 2];
+    JQC_REQUIRE(th == 64 || th == 128 || th == 256, JQC_ERR_INVALID, "jqc_set_tuning: threads must be 64, 128 or 256");
+    JQC_REQUIRE(lp >= 1 && lp <= (1 << 20), JQC_ERR_INVALID, "jqc_set_tuning: lane_prims out of range");
+    JQC_REQUIRE(pe == 0 || pe == 1, JQC_ERR_INVALID, "jqc_set_tuning: persistent must be 0 or 1");
+  }
+  bool chunks_changed = false;
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    if (c->tune[qc].lane_prims != cfg[3 * qc + 1]) chunks_changed = true;
+    c->tune[qc] = ClassTune{cfg[3 * qc], cfg[3 * qc + 1], cfg[3 * qc + 2]};
+  }
+  if (chunks_changed) drop_jk_tasks(c);  // the work lists depend on lane_prims
+  return JQC_OK;
+}
+
+// Workload signature for the tuning cache: device, precision settings and
+// the order of magnitude of the screened quartets of every class.
+static std::string tune_signature(jqc_ctx* c, const TaskSet* ts, int n_dens, int precision_mode, double dens_tau) {
+  cudaDeviceProp prop;
+  std::string sig = "jqc-tune1";
+  if (cudaGetDeviceProperties(&prop, c->device) == cudaSuccess) {
+    std::string name = prop.name;
+    for (char& ch : name)
+      if (ch == ' ' || ch == '\t') ch = '_';
+    sig += " dev=" + name + "/" + std::to_string(prop.multiProcessorCount);
+  }
+  sig += " mode=" + std::to_string(precision_mode) + " ndens=" + std::to_string(n_dens) +
+         " dscreen=" + std::to_string(dens_tau > 0.0 ? 1 : 0) + " q=";
   for (int prec = 0; prec < 2; ++prec)
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-      JKParams p;
-      p.tasks = c->jk_cur->d.ptr + c->jk_cur->off[prec][qc];
-      p.n_tasks = c->jk_cur->cnt[prec][qc];
-      if (p.n_tasks == 0) continue;
-      p.pairs = c->d_pairs.ptr;
-      p.pp = prec ? (const void*)c->d_ppf.ptr : (const void*)c->d_pp.ptr;
-      p.centres = c->d_centres.ptr;
-      p.ao = c->d_ao.ptr;
-      p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
-      p.boys_al = prec ? (const void*)c->boysA32 : (const void*)c->boysA64;
-      p.D = D;
-      p.J = J;
-      p.K = K;
-      p.n = n;
-      p.n_dens = n_dens;
-      p.dmax = dmax;
-      p.n_shell = c->n_shell;
-      p.dens_tau = (float)dens_tau;
-      if (class_ms) {
-        cudaEvent_t e0, e1;
-        JQC_CUDA_CHECK(cudaEventCreate(&e0));
-        JQC_CUDA_CHECK(cudaEventCreate(&e1));
-        JQC_CUDA_CHECK(cudaEventRecord(e0, s));
-        JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, s));
-        JQC_CUDA_CHECK(cudaEventRecord(e1, s));
-        JQC_CUDA_CHECK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        JQC_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-        class_ms[prec * kNumQuartetClasses + qc] = ms;
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-      } else {
-        JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, c->side[li++ % kNumStreams]));
+      const long long q = ts->class_quartets[prec][qc];
+      sig += std::to_string(q > 0 ? std::ilogb((double)q) + 1 : 0);
+      sig += (prec == 1 && qc == kNumQuartetClasses - 1) ? "" : ",";
+    }
+  return sig;
+}
+
+int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, int precision_mode, double mixed_tau,
+                 double dens_tau, const char* cache_path, int* from_cache, void* stream) {
+  JQC_REQUIRE(c && D && J && K, JQC_ERR_INVALID, "jqc_autotune: null argument");
+  JQC_REQUIRE(n_dens >= 1 && n_dens <= 4, JQC_ERR_INVALID, "jqc_autotune: n_dens must be 1..4");
+  JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_autotune: call jqc_pairs_build first");
+  JQC_REQUIRE(precision_mode >= 0 && precision_mode <= 2, JQC_ERR_INVALID, "jqc_autotune: bad precision_mode");
+  JQC_REQUIRE(mixed_tau >= 0.0 && dens_tau >= 0.0, JQC_ERR_INVALID, "jqc_autotune: thresholds must be >= 0");
+  int rc = select_device(c);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  JQC_REQUIRE(!stream_capturing(s), JQC_ERR_INVALID, "jqc_autotune: cannot run inside a graph capture");
+  if (from_cache) *from_cache = 0;
+  rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+  if (rc) return rc;
+  const std::string sig = tune_signature(c, c->jk_cur, n_dens, precision_mode, dens_tau);
+  int cfg[3 * kNumQuartetClasses];
+  // 1. cache hit: "signature<TAB>63 integers" per line
+  if (cache_path && cache_path[0]) {
+    std::FILE* f = std::fopen(cache_path, "r");
+    if (f) {
+      std::string line;
+      bool hit = false;
+      int ch;
+      while (!hit) {
+        line.clear();
+        while ((ch = std::fgetc(f)) != EOF && ch != '\n') line.push_back((char)ch);
+        const size_t tab = line.find('\t');
+        if (tab != std::string::npos && line.compare(0, tab, sig) == 0 && tab == sig.size()) {
+          const char* q = line.c_str() + tab + 1;
+          int k = 0;
+          char* end = nullptr;
+          for (; k < 3 * kNumQuartetClasses; ++k) {
+            const long v = std::strtol(q, &end, 10);
+            if (end == q) break;
+            cfg[k] = (int)v;
+            q = end;
+          }
+          hit = (k == 3 * kNumQuartetClasses);
+        }
+        if (ch == EOF) break;
+      }
+      std::fclose(f);
+      if (hit) {
+        rc = jqc_set_tuning(c, cfg);
+        if (rc) return rc;
+        rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+        if (rc) return rc;
+        if (from_cache) *from_cache = 1;
+        return JQC_OK;
       }
     }
-  for (int i = 0; i < kNumStreams; ++i) {
-    JQC_CUDA_CHECK(cudaEventRecord(c->ev_join[i], c->side[i]));
-    JQC_CUDA_CHECK(cudaStreamWaitEvent(s, c->ev_join[i], 0));
   }
-  JQC_CUDA_CHECK(launch_symmetrize(J, n_dens, n, s));
-  JQC_CUDA_CHECK(launch_symmetrize(K, n_dens, n, s));
+  float* dmax = nullptr;
+  if (dens_tau > 0.0) {
+    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
+    dmax = c->d_dmax.ptr;
+  }
+  // per-class time of the current settings: min over two timed builds
+  double ms[2 * kNumQuartetClasses], best_ms[kNumQuartetClasses];
+  auto time_classes = [&](double* per_class) -> int {
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) per_class[qc] = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {
+      int r = run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dens_tau, s, ms);
+      if (r) return r;
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc)
+        per_class[qc] = std::min(per_class[qc], ms[qc] + ms[kNumQuartetClasses + qc]);
+    }
+    return JQC_OK;
+  };
+  ClassTune best[kNumQuartetClasses];
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    best[qc] = ClassTune{};
+    best_ms[qc] = 1e300;
+  }
+  double cur[kNumQuartetClasses];
+  // 2. block size and grid form (no work-list rebuild needed)
+  const int th_opts[3] = {64, 128, 256};
+  for (int ti = 0; ti < 3; ++ti)
+    for (int pe = 0; pe < 2; ++pe) {
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+        c->tune[qc].threads = th_opts[ti];
+        c->tune[qc].persistent = pe;
+        c->tune[qc].lane_prims = kMaxLanePrims;
+      }
+      rc = time_classes(cur);
+      if (rc) return rc;
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc)
+        if (cur[qc] < best_ms[qc]) {
+          best_ms[qc] = cur[qc];
+          best[qc].threads = th_opts[ti];
+          best[qc].persistent = pe;
+        }
+    }
+  // 3. bra primitive chunk (work list rebuilt per value)
+  const int lp_opts[4] = {64, 128, 512, 1024};
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    c->tune[qc].threads = best[qc].threads;
+    c->tune[qc].persistent = best[qc].persistent;
+  }
+  for (int li = 0; li < 4; ++li) {
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->tune[qc].lane_prims = lp_opts[li];
+    drop_jk_tasks(c);
+    rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+    if (rc) return rc;
+    rc = time_classes(cur);
+    if (rc) return rc;
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc)
+      if (cur[qc] < best_ms[qc]) {
+        best_ms[qc] = cur[qc];
+        best[qc].lane_prims = lp_opts[li];
+      }
+  }
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+    if (!is_reg_class(qc)) {  // the warp engine has a fixed launch shape
+      best[qc].threads = 128;
+      best[qc].persistent = 0;
+    }
+    cfg[3 * qc] = best[qc].threads;
+    cfg[3 * qc + 1] = best[qc].lane_prims;
+    cfg[3 * qc + 2] = best[qc].persistent;
+  }
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->tune[qc].lane_prims = -1;  // force a rebuild
+  rc = jqc_set_tuning(c, cfg);
+  if (rc) return rc;
+  rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+  if (rc) return rc;
+  if (cache_path && cache_path[0]) {
+    std::FILE* f = std::fopen(cache_path, "a");
+    JQC_REQUIRE(f != nullptr, JQC_ERR_INVALID, "jqc_autotune: cannot open the cache file for appending");
+    std::fprintf(f, "%s\t", sig.c_str());
+    for (int k = 0; k < 3 * kNumQuartetClasses; ++k) std::fprintf(f, k ? " %d" : "%d", cfg[k]);
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
   return JQC_OK;
 }
 
@@ -973,43 +1332,7 @@ int jk_run_preallocated(jqc_ctx* c, int n_dens, const double* D, double* J, doub
               "with the same settings first, at a point where allocation is allowed");
   int rc = select_device(c);
   if (rc) return rc;
-  const int n = c->n_bf;
-  const size_t nn = (size_t)n * n * n_dens;
-  JQC_CUDA_CHECK(cudaMemsetAsync(J, 0, nn * sizeof(double), s));
-  JQC_CUDA_CHECK(cudaMemsetAsync(K, 0, nn * sizeof(double), s));
-  JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, dmax_scratch, s));
-  JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
-  for (int i = 0; i < kNumStreams; ++i) JQC_CUDA_CHECK(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
-  int li = 0;
-  for (int prec = 0; prec < 2; ++prec)
-    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-      JKParams p;
-      p.tasks = ts->d.ptr + ts->off[prec][qc];
-      p.n_tasks = ts->cnt[prec][qc];
-      if (p.n_tasks == 0) continue;
-      p.pairs = c->d_pairs.ptr;
-      p.pp = prec ? (const void*)c->d_ppf.ptr : (const void*)c->d_pp.ptr;
-      p.centres = c->d_centres.ptr;
-      p.ao = c->d_ao.ptr;
-      p.boys = prec ? (const void*)c->boys32 : (const void*)c->boys64;
-      p.boys_al = prec ? (const void*)c->boysA32 : (const void*)c->boysA64;
-      p.D = D;
-      p.J = J;
-      p.K = K;
-      p.n = n;
-      p.n_dens = n_dens;
-      p.dmax = dmax_scratch;
-      p.n_shell = c->n_shell;
-      p.dens_tau = (float)dens_tau;
-      JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, c->side[li++ % kNumStreams]));
-    }
-  for (int i = 0; i < kNumStreams; ++i) {
-    JQC_CUDA_CHECK(cudaEventRecord(c->ev_join[i], c->side[i]));
-    JQC_CUDA_CHECK(cudaStreamWaitEvent(s, c->ev_join[i], 0));
-  }
-  JQC_CUDA_CHECK(launch_symmetrize(J, n_dens, n, s));
-  JQC_CUDA_CHECK(launch_symmetrize(K, n_dens, n, s));
-  return JQC_OK;
+  return run_jk_set(c, ts, n_dens, D, J, K, dmax_scratch, dens_tau, s, nullptr);
 }
 
 }  // namespace jqc

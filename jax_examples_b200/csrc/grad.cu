@@ -379,6 +379,7 @@ __global__ void grad1e_st_kernel(const Grad1Params p) {
   if (idx >= npair) return;
   int i, j;
   pair_index(idx, i, j);
+  if (p.shell_mol && p.shell_mol[i] != p.shell_mol[j]) return;  // shells of two molecules of a batch
   const double fac = (i == j) ? 1.0 : 2.0;
   const int la = p.l[i], lb = p.l[j];
   const int na = ncart(la), nb = ncart(lb);
@@ -445,6 +446,8 @@ __global__ void grad1e_v_kernel(const Grad1Params p) {
   const int idx = (int)(gidx / p.n_atom), c = (int)(gidx % p.n_atom);
   int i, j;
   pair_index(idx, i, j);
+  // batch: the pair and the nucleus belong to one molecule
+  if (p.shell_mol && (p.shell_mol[i] != p.shell_mol[j] || p.atom_mol[c] != p.shell_mol[i])) return;
   const double fac = (i == j) ? 1.0 : 2.0;
   const int la = p.l[i], lb = p.l[j];
   const int na = ncart(la), nb = ncart(lb);

@@ -157,22 +157,47 @@ struct JKBody {
   }
 };
 
+// Warps walk the task list with a grid stride: one task per warp when the
+// grid covers the list, several (a persistent grid of resident blocks) when
+// the launch caps the grid.
 template <typename T, int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) jk_kernel(const JKParams prm) {
+__global__ void __launch_bounds__(kMaxJKThreads) jk_kernel(const JKParams prm) {
   constexpr int NS = class_split(LA, LB, LC, LD);
-  __shared__ T sE[4][3][LA + 1][LB + 1][LA + LB + 1];
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (warp >= prm.n_tasks) return;
-  JKBody<T, LA, LB, LC, LD, NS> body{prm, warp, int(threadIdx.x & 31), sE[threadIdx.x >> 5]};
-  dispatch_part<NS>(blockIdx.y, body);
+  __shared__ T sE[kMaxJKThreads / 32][3][LA + 1][LB + 1][LA + LB + 1];
+  const int stride = int((gridDim.x * blockDim.x) >> 5);
+  for (int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); warp < prm.n_tasks; warp += stride) {
+    JKBody<T, LA, LB, LC, LD, NS> body{prm, warp, int(threadIdx.x & 31), sE[threadIdx.x >> 5]};
+    dispatch_part<NS>(blockIdx.y, body);
+    __syncwarp();  // every lane is done with the warp's bra E before the next task writes it
+  }
 }
 
 template <typename T, int LA, int LB, int LC, int LD>
 cudaError_t launch_jk_class(const JKParams& p, cudaStream_t s) {
   constexpr int NS = class_split(LA, LB, LC, LD);
   if (p.n_tasks == 0) return cudaSuccess;
-  dim3 grid((p.n_tasks + 3) / 4, NS);
-  jk_kernel<T, LA, LB, LC, LD><<<grid, 128, 0, s>>>(p);
+  const int threads = (p.threads == 64 || p.threads == 256) ? p.threads : 128;
+  const int wpb = threads / 32;
+  long long blocks = (p.n_tasks + wpb - 1) / wpb;
+  if (p.persistent) {
+    // resident blocks per SM for this block size, times the SM count
+    static int occ[3] = {0, 0, 0};
+    static int sms = 0;
+    const int slot = threads == 64 ? 0 : (threads == 128 ? 1 : 2);
+    if (occ[slot] == 0) {
+      int dev = 0, o = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, jk_kernel<T, LA, LB, LC, LD>, threads, 0);
+      if (e != cudaSuccess) return e;
+      occ[slot] = o > 0 ? o : 1;
+    }
+    const long long cap = (long long)occ[slot] * sms;
+    if (blocks > cap) blocks = cap;
+  }
+  dim3 grid((unsigned)blocks, NS);
+  jk_kernel<T, LA, LB, LC, LD><<<grid, threads, 0, s>>>(p);
   return cudaGetLastError();
 }
 

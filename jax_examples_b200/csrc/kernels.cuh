@@ -30,7 +30,11 @@ struct JKParams {
   const float* dmax;       // n_shell x n_shell max |D| per shell block, or null
   int n_shell;
   float dens_tau;
+  int threads = 128;       // threads per block (64, 128, 256)
+  int persistent = 0;      // 1: grid capped at the resident blocks, warps stride over tasks
 };
+
+constexpr int kMaxJKThreads = 256;
 
 struct TensorParams {
   const Task* tasks;
@@ -120,6 +124,8 @@ struct Grad1Params {
   const int* atom;
   const double* atom_xyz;
   const double* atom_Z;
+  const int* shell_mol;  // molecule of each shell / atom (nullptr: one molecule)
+  const int* atom_mol;
   const double* boys;
   const double* D;
   const double* W;

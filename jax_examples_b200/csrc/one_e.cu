@@ -26,6 +26,8 @@ struct OneEParams {
   const int* ao;
   const double* atom_xyz;
   const double* atom_Z;
+  const int* shell_mol;  // molecule of each shell / atom (nullptr: one molecule)
+  const int* atom_mol;
   const double* boys;
   double* S;
   double* T;
@@ -47,7 +49,10 @@ __global__ void one_e_kernel(const OneEParams p) {
   double s[36], t[36], v[36];
   for (int x = 0; x < na * nb; ++x) s[x] = t[x] = v[x] = 0.0;
   const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
-  for (int ia = 0; ia < p.nprim[i]; ++ia)
+  // shells of different molecules of a batch: the block stays zero
+  const int mol = p.shell_mol ? p.shell_mol[i] : 0;
+  const int npa = (p.shell_mol && p.shell_mol[j] != mol) ? 0 : p.nprim[i];
+  for (int ia = 0; ia < npa; ++ia)
     for (int ib = 0; ib < p.nprim[j]; ++ib) {
       const double al = p.exps[p.prim_off[i] + ia], be = p.exps[p.prim_off[j] + ib];
       const double w = p.coefs[p.prim_off[i] + ia] * p.coefs[p.prim_off[j] + ib];
@@ -105,6 +110,7 @@ __global__ void one_e_kernel(const OneEParams p) {
       // nuclear attraction
       const int L = la + lb;
       for (int c = 0; c < p.n_atom; ++c) {
+        if (p.atom_mol && p.atom_mol[c] != mol) continue;  // nuclei of this molecule only
         const double X = P[0] - p.atom_xyz[3 * c], Y = P[1] - p.atom_xyz[3 * c + 1], Z = P[2] - p.atom_xyz[3 * c + 2];
         double F[kBoysMaxM + 1];
         boys_eval_rt<double>(pp * (X * X + Y * Y + Z * Z), p.boys, L, F);

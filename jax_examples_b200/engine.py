@@ -94,9 +94,14 @@ class DirectERI:
         schwarz_tau: shell quartets with Q_ij Q_kl below this are skipped.
         prim_tau: primitive pairs of magnitude below this are dropped
             (1e-20 changes no integral by more than ~1e-19).
+        mol_of_atom: optional molecule index of every atom when the basis
+            and nuclei are a batch of independent molecules
+            (``jqc_batch_partition``); matrices are then the block-diagonal
+            matrices of the whole batch.
     """
 
-    def __init__(self, basis, mol=None, device=None, schwarz_tau: float = 1e-13, prim_tau: float = 1e-20):
+    def __init__(self, basis, mol=None, device=None, schwarz_tau: float = 1e-13, prim_tau: float = 1e-20,
+                 mol_of_atom=None):
         self.device = _require_cuda(device)
         self.lib = _abi.load()
         self.basis = basis
@@ -120,6 +125,13 @@ class DirectERI:
                 "jqc_basis_upload", self._ctx, pk.n_shell, ip(pk.l), ip(pk.nprim), ip(pk.prim_off), dp(pk.exps),
                 dp(pk.coefs), dp(pk.centres), ip(pk.atom), len(self.atom_Z), dp(self.atom_xyz), dp(self.atom_Z), 1,
             )
+            self.n_mol = 1
+            if mol_of_atom is not None:
+                moa = np.ascontiguousarray(np.asarray(mol_of_atom, dtype=np.int32))
+                if moa.shape != (len(self.atom_Z),):
+                    raise ValueError(f"mol_of_atom must have one entry per atom ({len(self.atom_Z)})")
+                self.n_mol = int(moa.max()) + 1 if moa.size else 1
+                _abi.call("jqc_batch_partition", self._ctx, self.n_mol, ip(moa))
             _abi.call("jqc_pairs_build", self._ctx, self.schwarz_tau, float(prim_tau), _stream(self.device))
         self._C = None
         if pk.spherical:

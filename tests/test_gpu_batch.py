@@ -1,0 +1,226 @@
+"""Batched path on the GPU: one context over molecules of uneven size
+(jqc_batch_partition), CUDA-graph replay, per-class tuning and the autotuner,
+lock-step RHF, batched gradients and the batched BFGS.  Every batched result
+is checked against the same molecule run alone (itself pinned to the oracle
+in test_gpu_parity / test_gpu_gradient) and, for one small batch, against the
+oracle directly.  Tolerances: J/K 1e-10, energies 1e-8 Eh, gradients
+1e-7 Eh/bohr (the plain FP64 path's)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from jax_examples_b200 import CalcConfig, DirectERI, _abi, compute_integrals, run_scf
+from jax_examples_b200 import basis as pb
+from jax_examples_b200.batch import (BATCH_DENS_TAU, BatchedERI, MoleculeBatch, optimize_bfgs_batch,
+                                     rhf_gradient_batch, run_rhf_batch)
+from jax_examples_b200.grad import rhf_gradient
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+BASIS = "syn-6-31g*"
+
+
+def _mols(sizes, seed=0, noise=0.05):
+    return [pb.water_cluster(n, seed=seed + i, noise_angstrom=noise) for i, n in enumerate(sizes)]
+
+
+def _random_block_density(batch, rng, scale=0.05):
+    n = batch.n_basis
+    D = np.zeros((n, n))
+    for m in range(len(batch)):
+        o, k = batch.bf_off[m], batch.n_bf[m]
+        a = rng.standard_normal((k, k)) * scale
+        D[o:o + k, o:o + k] = a + a.T
+    return D
+
+
+def test_batch_jk_matches_each_molecule_alone():
+    batch = MoleculeBatch(_mols([1, 3, 2]), BASIS)
+    eng = BatchedERI(batch, schwarz_tau=1e-12)
+    rng = np.random.default_rng(3)
+    D = torch.tensor(_random_block_density(batch, rng), device=DEV)[None].contiguous()
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    eng.jk_into(D, J, K)
+    torch.cuda.synchronize()
+    Jn, Kn = J[0].cpu().numpy(), K[0].cpu().numpy()
+    mask = np.zeros_like(Jn, dtype=bool)
+    for m, mol in enumerate(batch.mols):
+        o, k = batch.bf_off[m], batch.n_bf[m]
+        mask[o:o + k, o:o + k] = True
+        single = DirectERI(batch.bases[m], mol, device=0, schwarz_tau=1e-12)
+        Js, Ks = single.jk(D[0, o:o + k, o:o + k].contiguous())
+        np.testing.assert_allclose(Jn[o:o + k, o:o + k], Js.cpu().numpy(), atol=1e-10, rtol=0)
+        np.testing.assert_allclose(Kn[o:o + k, o:o + k], Ks.cpu().numpy(), atol=1e-10, rtol=0)
+        single.close()
+    assert np.all(Jn[~mask] == 0.0) and np.all(Kn[~mask] == 0.0)
+    eng.close()
+
+
+def test_batch_jk_vs_oracle_small():
+    mols = [pb.water_cluster(1, seed=1, noise_angstrom=0.05), pb.water_cluster(1, seed=2, noise_angstrom=0.05)]
+    batch = MoleculeBatch(mols, "syn-sto-3g")
+    eng = BatchedERI(batch, schwarz_tau=0.0)
+    rng = np.random.default_rng(5)
+    Dn = _random_block_density(batch, rng)
+    D = torch.tensor(Dn, device=DEV)[None].contiguous()
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    eng.jk_into(D, J, K)
+    for m in range(2):
+        o, k = batch.bf_off[m], batch.n_bf[m]
+        eri = oracle.eri_tensor(batch.bases[m])
+        Jr, Kr = oracle.jk_from_tensor(np.ascontiguousarray(Dn[o:o + k, o:o + k]), eri)
+        np.testing.assert_allclose(J[0, o:o + k, o:o + k].cpu().numpy(), Jr, atol=1e-10, rtol=0)
+        np.testing.assert_allclose(K[0, o:o + k, o:o + k].cpu().numpy(), Kr, atol=1e-10, rtol=0)
+    eng.close()
+
+
+def test_batch_one_electron_matches_each_molecule():
+    batch = MoleculeBatch(_mols([2, 1]), BASIS)
+    eng = BatchedERI(batch)
+    S, T, V = (x.cpu().numpy() for x in eng.engine.one_electron())
+    for m, mol in enumerate(batch.mols):
+        o, k = batch.bf_off[m], batch.n_bf[m]
+        ints = compute_integrals(mol, batch.bases[m], device=0)
+        np.testing.assert_allclose(S[o:o + k, o:o + k], np.asarray(ints.S.cpu()), atol=1e-12, rtol=0)
+        np.testing.assert_allclose(T[o:o + k, o:o + k], np.asarray(ints.T.cpu()), atol=1e-12, rtol=0)
+        np.testing.assert_allclose(V[o:o + k, o:o + k], np.asarray(ints.V.cpu()), atol=1e-11, rtol=0)
+    o1 = batch.bf_off[1]
+    assert np.all(S[:o1, o1:] == 0.0) and np.all(V[:o1, o1:] == 0.0)
+    eng.close()
+
+
+def test_graph_replay_matches_eager_and_follows_buffer_contents():
+    batch = MoleculeBatch(_mols([2, 4, 1]), BASIS)
+    eng = BatchedERI(batch)
+    rng = np.random.default_rng(9)
+    D, J, K = eng.buffers(1)
+    D[0].copy_(torch.tensor(_random_block_density(batch, rng), device=DEV))
+    gid = eng.capture_jk(D, J, K, "fp64", dens_tau=BATCH_DENS_TAU)
+    for trial in range(2):
+        D[0].copy_(torch.tensor(_random_block_density(batch, rng), device=DEV))
+        J.fill_(float("nan"))
+        K.fill_(float("nan"))
+        eng.launch(gid)
+        J2, K2 = torch.empty_like(J), torch.empty_like(K)
+        eng.jk_into(D, J2, K2, "fp64", dens_tau=BATCH_DENS_TAU)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(J.cpu().numpy(), J2.cpu().numpy(), atol=1e-11, rtol=0)
+        np.testing.assert_allclose(K.cpu().numpy(), K2.cpu().numpy(), atol=1e-11, rtol=0)
+    # a new work list (different bra chunking) destroys the graph
+    cfg = eng.tuning()
+    cfg[:, 1] = 64
+    eng.set_tuning(cfg)
+    with pytest.raises(ValueError, match="invalidated"):
+        eng.launch(gid)
+    eng.close()
+
+
+def test_capture_requires_prebuilt_work_list_and_created_stream():
+    batch = MoleculeBatch(_mols([1]), BASIS)
+    eng = BatchedERI(batch)
+    D, J, K = eng.buffers(1)
+    with pytest.raises(ValueError, match="legacy default stream"):
+        _abi.call("jqc_graph_begin", eng.engine._ctx, None)
+    s = torch.cuda.Stream()
+    import ctypes
+
+    sp = ctypes.c_void_p(s.cuda_stream)
+    s.wait_stream(torch.cuda.current_stream())
+    _abi.call("jqc_graph_begin", eng.engine._ctx, sp)
+    with pytest.raises(_abi.JQCError, match="before the capture"):
+        eng.jk_into(D, J, K, "fp32", stream=s)  # no FP32 work list yet
+    gid = ctypes.c_int(-1)
+    rc = eng.engine.lib.jqc_graph_end(eng.engine._ctx, sp, ctypes.byref(gid))
+    if rc == 0:
+        eng.engine.lib.jqc_graph_destroy(eng.engine._ctx, gid.value)
+    torch.cuda.synchronize()
+    eng.close()
+
+
+@pytest.mark.parametrize("threads,persistent,lane_prims", [(64, 1, 64), (256, 0, 1024), (256, 1, 128)])
+def test_launch_shapes_give_same_jk(threads, persistent, lane_prims):
+    batch = MoleculeBatch(_mols([3, 2]), BASIS)
+    eng = BatchedERI(batch)
+    rng = np.random.default_rng(4)
+    D = torch.tensor(_random_block_density(batch, rng), device=DEV)[None].contiguous()
+    J0, K0 = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J0, K0)
+    cfg = eng.tuning()
+    assert cfg.shape == (21, 3) and np.all(cfg[:, 0] == 128)
+    cfg[:, 0], cfg[:, 1], cfg[:, 2] = threads, lane_prims, persistent
+    eng.set_tuning(cfg)
+    np.testing.assert_array_equal(eng.tuning(), cfg)
+    J, K = torch.empty_like(D), torch.empty_like(D)
+    for prec in ("fp64", "mixed"):
+        eng.jk_into(D, J, K, prec, mixed_tau=1e-7)
+        torch.cuda.synchronize()
+        tol = 1e-10 if prec == "fp64" else 1e-6
+        np.testing.assert_allclose(J.cpu().numpy(), J0.cpu().numpy(), atol=tol, rtol=0)
+        np.testing.assert_allclose(K.cpu().numpy(), K0.cpu().numpy(), atol=tol, rtol=0)
+    bad = cfg.copy()
+    bad[0, 0] = 96
+    with pytest.raises(ValueError, match="threads"):
+        eng.set_tuning(bad)
+    eng.close()
+
+
+def test_autotune_keeps_results_and_uses_cache(tmp_path):
+    batch = MoleculeBatch(_mols([4, 2, 1]), BASIS)
+    eng = BatchedERI(batch)
+    rng = np.random.default_rng(6)
+    D = torch.tensor(_random_block_density(batch, rng), device=DEV)[None].contiguous()
+    J0, K0 = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J0, K0)
+    cache = str(tmp_path / "tune.txt")
+    J, K = torch.empty_like(D), torch.empty_like(D)
+    assert eng.autotune(D, J, K, "fp64", dens_tau=0.0, cache_path=cache) is False
+    tuned = eng.tuning()
+    assert set(np.unique(tuned[:, 0])) <= {64, 128, 256}
+    eng.jk_into(D, J, K)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(J.cpu().numpy(), J0.cpu().numpy(), atol=1e-10, rtol=0)
+    np.testing.assert_allclose(K.cpu().numpy(), K0.cpu().numpy(), atol=1e-10, rtol=0)
+    lines = open(cache).read().strip().splitlines()
+    assert len(lines) == 1 and len(lines[0].split("\t")[1].split()) == 63
+    eng.close()
+    eng2 = BatchedERI(batch)
+    assert eng2.autotune(D, J, K, "fp64", dens_tau=0.0, cache_path=cache) is True
+    np.testing.assert_array_equal(eng2.tuning(), tuned)
+    eng2.close()
+
+
+def test_rhf_batch_energies_and_gradients_match_single_runs():
+    mols = _mols([1, 3, 2], seed=11, noise=0.1)
+    batch = MoleculeBatch(mols, BASIS)
+    cfg = CalcConfig(scf_conv=1e-10, schwarz_tau=1e-12)
+    scf = run_rhf_batch(batch, cfg, use_graph=True)
+    grads = rhf_gradient_batch(batch, scf)
+    assert scf.record["graph"] and scf.record["fock_builds"] >= 2
+    for m, mol in enumerate(mols):
+        res_b = scf.results[m]
+        assert res_b.converged
+        ints = compute_integrals(mol, batch.bases[m], device=0, schwarz_tau=1e-12)
+        res = run_scf(mol, ints, CalcConfig(scf_conv=1e-10, schwarz_tau=1e-12))
+        assert abs(res_b.energy - res.energy) < 1e-8
+        g = rhf_gradient(mol, res, batch.bases[m])
+        np.testing.assert_allclose(grads[m].cpu().numpy(), g.cpu().numpy(), atol=1e-7, rtol=0)
+    scf.engine.close()
+
+
+def test_bfgs_batch_matches_single_molecule_runs():
+    mols = [pb.water_cluster(1, seed=21, noise_angstrom=0.1), pb.water_cluster(2, seed=22, noise_angstrom=0.1)]
+    both = optimize_bfgs_batch(mols, BASIS, max_steps=3)
+    for m, mol in enumerate(mols):
+        alone = optimize_bfgs_batch([mol], BASIS, max_steps=3)[0]
+        assert both[m].n_steps == alone.n_steps
+        e_b = np.array([e for _, e in both[m].trajectory])
+        e_a = np.array([e for _, e in alone.trajectory])
+        np.testing.assert_allclose(e_b, e_a, atol=1e-8, rtol=0)
+        assert np.all(np.diff(e_b) <= 1e-10)  # Armijo steps never raise the energy
