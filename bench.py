@@ -41,6 +41,10 @@ sys.path.insert(0, ROOT)
 N_WATERS = int(os.environ.get("JQC_BENCH_WATERS", "16"))
 BASIS = "syn-6-31g*"
 SCHWARZ_TAU = 1e-12
+# density-screening threshold of the chosen (mixed) path's gradient: skipped
+# quartets change the (H2O)16 gradient by ~2e-7 Eh/bohr, inside the 1e-5
+# tolerance of the mixed path
+CHOSEN_GRAD_TAU = 1e-10
 METRIC = "ERI quartets/s (direct J/K Fock build, (H2O)16 6-31G*-shaped)"
 WORKLOAD = (f"(H2O){N_WATERS} lattice 2.9A, 6-31G*-shaped Cartesian ({19 * N_WATERS} bf), "
             "FP64 direct J/K build")
@@ -148,6 +152,110 @@ class Clocks:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
                 "samples": len(rows)}
+
+
+def batched_sweep(local: int, n_mol: int, seed: int = 2024):
+    """Uneven-size geometry sweep: n_mol water clusters (1..12 waters,
+    +-0.1 A Gaussian noise) through one batched, autotuned, graph-replayed
+    RHF + gradient, against the same molecules one at a time on the plain
+    FP64 path (the reference's per-geometry loop shape)."""
+    import torch
+
+    from jax_examples_b200 import CalcConfig, DirectERI, compute_integrals, run_scf
+    from jax_examples_b200 import basis as pb
+    from jax_examples_b200.batch import MoleculeBatch, rhf_gradient_batch, run_rhf_batch
+    from jax_examples_b200.grad import rhf_gradient
+
+    rng = np.random.default_rng(seed)
+    sizes = [int(x) for x in rng.integers(1, 13, n_mol)]
+    mols = [pb.water_cluster(n, seed=seed + i, noise_angstrom=0.1) for i, n in enumerate(sizes)]
+    cfg = CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch = MoleculeBatch(mols, BASIS)
+    scf = run_rhf_batch(batch, cfg, use_graph=True, autotune=True)
+    timing = {}
+    grads = rhf_gradient_batch(batch, scf, timing)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    rec = scf.record
+    scf.engine.close()
+    fock_seq = grad_seq = 0.0
+    e_err = g_err = 0.0
+    iters = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m, mol in enumerate(mols):
+        eng = DirectERI(batch.bases[m], mol, device=local, schwarz_tau=SCHWARZ_TAU)
+        ints = compute_integrals(mol, batch.bases[m], device=local, engine=eng)
+        r = run_scf(mol, ints, cfg)
+        fock_seq += r.precision["jk_seconds"]
+        iters.append(r.n_iterations)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g = rhf_gradient(mol, r, engine=eng)
+        e1.record()
+        e1.synchronize()
+        grad_seq += e0.elapsed_time(e1) * 1e-3
+        e_err = max(e_err, abs(r.energy - scf.results[m].energy))
+        g_err = max(g_err, float((g - grads[m]).abs().max()))
+        eng.close()
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    return {
+        "workload": f"{n_mol} water clusters, 1..12 waters (seeded), +-0.1 A noise, {BASIS}",
+        "n_basis_total": batch.n_basis, "waters_total": int(sum(sizes)),
+        "batched": {"fock_s": round(rec["jk_seconds"], 4), "gradient_s": round(timing["grad_seconds"], 4),
+                    "fock_builds": rec["fock_builds"], "setup_s": round(rec["setup_seconds"], 3),
+                    "wall_s": round(t_batch, 3), "graph": rec["graph"], "autotuned": rec["autotuned"]},
+        "sequential_fp64": {"fock_s": round(fock_seq, 4), "gradient_s": round(grad_seq, 4),
+                            "iterations_mean": float(np.mean(iters)), "wall_s": round(t_seq, 3)},
+        "fock_plus_gradient_speedup": round((fock_seq + grad_seq) / max(1e-12, rec["jk_seconds"]
+                                                                         + timing["grad_seconds"]), 3),
+        "wall_speedup": round(t_seq / max(1e-12, t_batch), 3),
+        "max_energy_diff_eh": e_err, "max_gradient_diff_eh_bohr": g_err,
+    }
+
+
+def gradient_only(args):
+    """ERI-derivative adjoint alone (the profiling case of the gradient
+    kernels): core-guess density of the workload, --warmup untimed and
+    --steps timed jqc_grad2e calls; prints per-class kernel times."""
+    import torch
+
+    from jax_examples_b200 import DirectERI
+    from jax_examples_b200 import basis as pb
+    from jax_examples_b200.engine import QUARTET_CLASSES
+    from jax_examples_b200.grad import grad_two_electron
+
+    mol = pb.water_cluster(N_WATERS, seed=0)
+    bs = pb.build_basis_set(mol, BASIS)
+    eng = DirectERI(bs, mol, device=0, schwarz_tau=SCHWARZ_TAU)
+    S, T, V = eng.one_electron()
+    w, U = torch.linalg.eigh(S)
+    X = (U * (1.0 / torch.sqrt(w))[None, :]) @ U.T
+    _, Cp = torch.linalg.eigh(X.T @ (T + V) @ X)
+    C = X @ Cp
+    nocc = mol.n_electrons // 2
+    D = (2.0 * C[:, :nocc] @ C[:, :nocc].T).contiguous()
+    for _ in range(max(1, args.warmup)):
+        grad_two_electron(eng, [D], 1.0, 0.5)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        grad_two_electron(eng, [D], 1.0, 0.5)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = []
+    grad_two_electron(eng, [D], 1.0, 0.5, 0.0, ms)
+    print(json.dumps({"workload": WORKLOAD.replace("J/K build", "ERI-derivative adjoint"),
+                      "gradient_ms": float(np.mean(times)),
+                      "classes_ms": {"(%d%d|%d%d)" % QUARTET_CLASSES[q]: round(ms[q], 3) for q in range(21) if ms[q]}}))
 
 
 def run_ours(args):
@@ -280,7 +388,8 @@ def run_ours(args):
         ints = compute_integrals(mol, bs, device=local, engine=eng)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r64 = run_scf(mol, ints, CalcConfig(scf_conv=1e-8))
+        # plain: a full FP64 build every iteration (the reference's Fock build)
+        r64 = run_scf(mol, ints, CalcConfig(scf_conv=1e-8, incremental=False))
         torch.cuda.synchronize()
         t64 = time.perf_counter() - t0
         cfg = CalcConfig(scf_conv=1e-8, precision="mixed", incremental=True)
@@ -300,16 +409,32 @@ def run_ours(args):
         ge1.record()
         torch.cuda.synchronize()
         tgrad = ge0.elapsed_time(ge1) * 1e-3
-        gmx = rhf_gradient(mol, rmx, engine=eng)
+        rhf_gradient(mol, rmx, engine=eng, dens_tau=CHOSEN_GRAD_TAU)  # warm-up
+        torch.cuda.synchronize()
+        ge0.record()
+        gmx = rhf_gradient(mol, rmx, engine=eng, dens_tau=CHOSEN_GRAD_TAU)
+        ge1.record()
+        torch.cuda.synchronize()
+        tgrad_mx = ge0.elapsed_time(ge1) * 1e-3
+        plain_total = r64.precision["jk_seconds"] + tgrad
+        chosen_total = rmx.precision["jk_seconds"] + tgrad_mx
         fg = {"plain_fp64_scf_s": round(t64, 4), "plain_fp64_fock_s": round(r64.precision["jk_seconds"], 4),
-              "gradient_s": round(tgrad, 4),
+              "gradient_s": round(tgrad, 4), "chosen_gradient_s": round(tgrad_mx, 4),
+              "chosen_gradient_dens_tau": CHOSEN_GRAD_TAU,
               "gradient_err_eh_bohr": float((g64 - gmx).abs().max()),
+              "plain_fock_plus_gradient_s": round(plain_total, 4),
+              "chosen_fock_plus_gradient_s": round(chosen_total, 4),
+              "fock_plus_gradient_speedup": round(plain_total / max(1e-12, chosen_total), 3),
               "plain_iterations": r64.n_iterations, "chosen_scf_s": round(tmx, 4),
               "chosen_fock_s": round(rmx.precision["jk_seconds"], 4), "chosen_iterations": rmx.n_iterations,
               "chosen_builds": {k: rmx.precision[k] for k in ("builds_mixed", "builds_fp64", "incremental_builds")},
               "energy_fp64": r64.energy, "energy_chosen": rmx.energy,
               "energy_err_eh": abs(r64.energy - rmx.energy),
               "fock_speedup": round(r64.precision["jk_seconds"] / max(1e-12, rmx.precision["jk_seconds"]), 3)}
+
+    sweep = None
+    if world == 1 and args.batch_molecules > 0:
+        sweep = batched_sweep(local, args.batch_molecules)
 
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -337,6 +462,7 @@ def run_ours(args):
         "clocks": clk.summary(local),
         "cpu_baseline": cpu,
         "fock_gradient": fg,
+        "batched_sweep": sweep,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -354,7 +480,11 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-scf", dest="scf", action="store_false")
+    ap.add_argument("--batch-molecules", type=int, default=64,
+                    help="molecules in the batched uneven-size sweep (0 skips it)")
     ap.add_argument("--waters", type=int, default=None, help="cluster size (default 16; profiling uses smaller)")
+    ap.add_argument("--gradient-only", action="store_true",
+                    help="time only the ERI-derivative adjoint (profiling case)")
     args = ap.parse_args()
     if args.waters is not None:
         global N_WATERS, WORKLOAD
@@ -362,6 +492,8 @@ def main():
         WORKLOAD = WORKLOAD.replace("(H2O)16", f"(H2O){N_WATERS}").replace("(304 bf)", f"({19 * N_WATERS} bf)")
     if args.impl == "reference":
         run_reference(args)
+    elif args.gradient_only:
+        gradient_only(args)
     else:
         run_ours(args)
 

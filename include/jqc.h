@@ -130,6 +130,15 @@ int jqc_one_electron(jqc_ctx *ctx, double *S, double *T, double *V, void *stream
 int jqc_grad2e(jqc_ctx *ctx, int n_dens, const double *D, double j_scale, double k_scale, double *grad,
                void *stream);
 
+/* jqc_grad2e with density screening and per-class timing: quartets whose
+ * bound Q_ab Q_cd |Gamma|max is below dens_tau (0 = off) are skipped, with
+ * |Gamma|max <= j n^2 m_ab m_cd + (k/2) n (m_ac m_bd + m_ad m_bc) from the
+ * per-shell-block density maxima m over the n = n_dens densities.  With
+ * class_ms (21 doubles, or NULL) the classes are timed one by one with CUDA
+ * events (milliseconds, synchronizes).  No reference counterpart. */
+int jqc_grad2e_ex(jqc_ctx *ctx, int n_dens, const double *D, double j_scale, double k_scale, double dens_tau,
+                  double *grad, void *stream, double *class_ms);
+
 /* One-electron part of the nuclear gradient, ADDED into grad:
  * grad += sum D_ab d(T+V)_ab/dR - sum W_ab dS_ab/dR (Hellmann-Feynman term of
  * V included); D total density, W energy-weighted density (n x n, device).
@@ -185,21 +194,32 @@ int jqc_graph_end(jqc_ctx *ctx, void *stream, int *graph_id);
 int jqc_graph_launch(jqc_ctx *ctx, int graph_id, void *stream);
 int jqc_graph_destroy(jqc_ctx *ctx, int graph_id);
 
-/* Launch shape of each of the 21 quartet classes, cfg[3q..3q+2] = threads
- * per block (64/128/256), lane_prims (at most that many primitive quartets
- * per lane and task: the bra primitive pairs of a quartet are split into
- * chunks accordingly) and persistent (1: grid capped at the resident blocks,
- * warps stride over the task list).  Warp-engine classes use only
- * lane_prims.  Setting a new lane_prims rebuilds the work lists.  No
- * reference counterpart. */
-int jqc_get_tuning(jqc_ctx *ctx, int *cfg63);
-int jqc_set_tuning(jqc_ctx *ctx, const int *cfg63);
+/* Launch shape of each of the 21 quartet classes, cfg[4q..4q+3] =
+ * threads per block (64/128/256), lane_prims (at most that many primitive
+ * quartets per lane and task: the bra primitive pairs of a quartet are split
+ * into chunks accordingly), persistent (1: grid capped at the resident
+ * blocks, warps stride over the task list) and engine (0: register kernels,
+ * lane = ket shell pair, classes with L <= 6; 1: column engine, one warp per
+ * quartet, lane = ket Cartesian pair, classes with L >= 5; 2: runtime-class
+ * warp engine, every class).  threads and persistent apply to the register
+ * kernels only.  A new lane_prims or a change to or from the register engine
+ * rebuilds the work lists.  No reference counterpart. */
+int jqc_get_tuning(jqc_ctx *ctx, int *cfg84);
+int jqc_set_tuning(jqc_ctx *ctx, const int *cfg84);
+
+/* Engine of the ERI-derivative adjoint for one quartet class: 0 register
+ * kernels (L <= 4), 1 row engine (bra pair dp or dd; one warp per quartet,
+ * lane = bra Cartesian pair), 2 runtime-class warp engine.  Defaults: row
+ * engine for L >= 5, register kernels up to L = 4.  No reference
+ * counterpart. */
+int jqc_set_grad_engine(jqc_ctx *ctx, int quartet_class, int engine);
+int jqc_get_grad_engine(jqc_ctx *ctx, int *engines21);
 
 /* Autotuner: times every class of the J/K build for this density, precision
- * and screening (classes serialised, CUDA events, best of two) over threads
- * x persistent, then over lane_prims, keeps the fastest shape per class and
- * rebuilds the work list with it.  With cache_path, a line
- * "signature<TAB>63 integers" is appended; a later call whose signature
+ * and screening (classes serialised, CUDA events, best of two) over the
+ * engines, then threads x persistent, then lane_prims, keeps the fastest
+ * shape per class and rebuilds the work list with it.  With cache_path, a
+ * line "signature<TAB>84 integers" is appended; a later call whose signature
  * (device, settings, order of magnitude of each class's quartet count)
  * matches a line applies it without timing and sets *from_cache = 1.
  * J and K are overwritten.  Synchronizes.  No reference counterpart. */

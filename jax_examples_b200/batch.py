@@ -218,13 +218,15 @@ class BatchedERI:
         return bool(hit.value)
 
     def tuning(self) -> np.ndarray:
-        """(21, 3) array of (threads, lane_prims, persistent) per quartet class."""
-        out = np.zeros(63, dtype=np.int32)
+        """(21, 4) array of (threads, lane_prims, persistent, engine) per
+        quartet class; engine 0 register kernels, 1 column engine, 2 warp
+        engine."""
+        out = np.zeros(84, dtype=np.int32)
         _abi.call("jqc_get_tuning", self.engine._ctx, out.ctypes.data_as(_abi._ip))
-        return out.reshape(21, 3)
+        return out.reshape(21, 4)
 
     def set_tuning(self, cfg) -> None:
-        arr = np.ascontiguousarray(np.asarray(cfg, dtype=np.int32).reshape(63))
+        arr = np.ascontiguousarray(np.asarray(cfg, dtype=np.int32).reshape(84))
         _abi.call("jqc_set_tuning", self.engine._ctx, arr.ctypes.data_as(_abi._ip))
 
 

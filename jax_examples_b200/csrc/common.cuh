@@ -32,6 +32,7 @@ void set_error(const std::string& msg);
     cudaError_t _e = (expr);                                                      \
     if (_e != cudaSuccess) {                                                      \
       ::jqc::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));       \
+      (void)cudaGetLastError(); /* reported here: not again by a later launch */ \
       return JQC_ERR_CUDA;                                                        \
     }                                                                             \
   } while (0)

@@ -52,7 +52,8 @@ cudaError_t launch_jk64_hi(int qc, const JKParams& p, cudaStream_t s);
 cudaError_t launch_jk32_lo(int qc, const JKParams& p, cudaStream_t s);
 cudaError_t launch_jk32_hi(int qc, const JKParams& p, cudaStream_t s);
 cudaError_t launch_jk(int qc, bool fp32, const JKParams& p, cudaStream_t s) {
-  if (!is_reg_class(qc)) {
+  if (p.engine == kEngineCol) return launch_col_jk(qc, fp32, p, s);
+  if (p.engine == kEngineWarp || !is_reg_class(qc)) {
     const int pb = qc_bra(qc), pk = qc_ket(qc);
     return launch_warp_jk(pc_la(pb), pc_lb(pb), pc_la(pk), pc_lb(pk), fp32, p, s);
   }
@@ -183,6 +184,7 @@ struct Block {
 
 // Upper bound on primitive quartets one lane evaluates per task (default).
 constexpr int kMaxLanePrims = 256;
+constexpr int kTuneInts = 4;  // threads, lane_prims, persistent, engine
 
 // Launch shape of one quartet class, picked by the autotuner: threads per
 // block, the bra primitive-pair chunk (at most lane_prims primitive quartets
@@ -191,7 +193,30 @@ struct ClassTune {
   int threads = 128;
   int lane_prims = kMaxLanePrims;
   int persistent = 0;
+  int engine = -1;  // JKEngine; -1: the class's default
 };
+
+// Default engine of a class: the register kernels where they exist, else the
+// column engine, else the runtime-class warp engine.
+static int default_engine(int qc) {
+  if (qc == 19 || qc == 20) return has_col_class(qc) ? kEngineCol : kEngineWarp;
+  return is_reg_class(qc) ? kEngineReg : (has_col_class(qc) ? kEngineCol : kEngineWarp);
+}
+static int class_engine(const ClassTune& t, int qc) { return t.engine < 0 ? default_engine(qc) : t.engine; }
+
+// Gradient: the row engine for the d-bra classes at L >= 5, the register
+// kernels up to L = 4, the warp engine otherwise.
+static int default_grad_engine(int qc) {
+  if (has_grad_row_class(qc) && qc_L(qc) >= 5) return kEngineCol;
+  return is_grad_reg_class(qc) ? kEngineReg : kEngineWarp;
+}
+static bool grad_engine_valid(int e, int qc) {
+  return (e == kEngineReg && is_grad_reg_class(qc)) || (e == kEngineCol && has_grad_row_class(qc)) ||
+         e == kEngineWarp;
+}
+static bool engine_valid(int e, int qc) {
+  return (e == kEngineReg && is_reg_class(qc)) || (e == kEngineCol && has_col_class(qc)) || e == kEngineWarp;
+}
 constexpr int kNumStreams = 4;
 
 }  // namespace jqc
@@ -229,6 +254,7 @@ struct jqc_ctx {
   TaskSet grad_tasks;  // one screened quartet per task, whole contractions
   // scratch
   DevBuf<float> d_dmax;
+  DevBuf<double> d_pair_force;  // gradient: 6 force components per kept shell pair
   cudaStream_t side[kNumStreams] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kNumStreams] = {};
   cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // per-class timing
@@ -238,6 +264,7 @@ struct jqc_ctx {
   const float* boysA32 = nullptr;
   double prim_tau = 0.0;
   ClassTune tune[kNumQuartetClasses];
+  int grad_engine[kNumQuartetClasses];  // JKEngine numbering: 0 register, 1 row engine, 2 warp
   // CUDA graphs captured through jqc_graph_begin / jqc_graph_end
   std::vector<cudaGraphExec_t> graphs;
 };
@@ -316,10 +343,11 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
         // primitive quartets per task (the tensor keeps whole quartets).
         const int nbp = c->pairs[gi].npp, nkp = K.ka * K.kb;
         int chunk = nbp;
-        if (!full && !grad) chunk = std::max(1, std::min(nbp, c->tune[qc].lane_prims / std::max(1, nkp)));
+        if (!full) chunk = std::max(1, std::min(nbp, c->tune[qc].lane_prims / std::max(1, nkp)));
         // Register classes: 32 kets per warp task (one per lane).  Warp-engine
         // classes: one ket per task, so every quartet gets its own warp.
-        const int per_task = grad ? (is_grad_reg_class(qc) ? 32 : 1) : (is_reg_class(qc) ? 32 : 1);
+        const int per_task =
+            grad ? (c->grad_engine[qc] == kEngineReg ? 32 : 1) : (class_engine(c->tune[qc], qc) == kEngineReg ? 32 : 1);
         for (int prec = 0; prec < 2; ++prec) {
           for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
             for (int b0 = 0; b0 < nbp; b0 += chunk) {
@@ -481,6 +509,7 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
       p.dens_tau = (float)dens_tau;
       p.threads = c->tune[qc].threads;
       p.persistent = c->tune[qc].persistent;
+      p.engine = class_engine(c->tune[qc], qc);
       if (class_ms) {
         JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));
         JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, s));
@@ -528,6 +557,7 @@ int jqc_ctx_create(int device, jqc_ctx** out) {
     delete c;
     return rc;
   }
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->grad_engine[qc] = default_grad_engine(qc);
   c->boys64 = bt.t64;
   c->boys32 = bt.t32;
   c->boysA64 = bt.a64;
@@ -559,10 +589,9 @@ int jqc_ctx_destroy(jqc_ctx* ctx) {
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_t0) cudaEventDestroy(ctx->ev_t0);
     if (ctx->ev_t1) cudaEventDestroy(ctx->ev_t1);
-    for (cudaGraphExec_t g : ctx->graphs)
-      if (g) cudaGraphExecDestroy(g);
-    drop_jk_tasks(ctx);
+    drop_jk_tasks(ctx);  // destroys the captured graphs too
     delete ctx;
+    (void)cudaGetLastError();  // teardown status is not reported to later calls
   }
   return JQC_OK;
 }
@@ -918,21 +947,39 @@ int jqc_eri_tensor(jqc_ctx* c, double* out, long long max_bytes, void* stream) {
   return JQC_OK;
 }
 
-int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k_scale, double* grad,
-               void* stream) {
+int jqc_grad2e_ex(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k_scale, double dens_tau,
+                  double* grad, void* stream, double* class_ms) {
   JQC_REQUIRE(c && D && grad, JQC_ERR_INVALID, "jqc_grad2e: null argument");
   JQC_REQUIRE(n_dens >= 1 && n_dens <= 4, JQC_ERR_INVALID, "jqc_grad2e: n_dens must be 1..4");
   JQC_REQUIRE(c->pairs_ready, JQC_ERR_NOT_READY, "jqc_grad2e: call jqc_pairs_build first");
   JQC_REQUIRE(c->n_atom > 0, JQC_ERR_NOT_READY, "jqc_grad2e: the basis was uploaded without atoms");
+  JQC_REQUIRE(dens_tau >= 0.0 && std::isfinite(dens_tau), JQC_ERR_INVALID, "jqc_grad2e: dens_tau must be >= 0");
   int rc = select_device(c);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  JQC_REQUIRE(c->grad_tasks.valid || !stream_capturing(s), JQC_ERR_NOT_READY,
+  const bool capturing = stream_capturing(s);
+  JQC_REQUIRE(!(capturing && class_ms), JQC_ERR_INVALID, "jqc_grad2e_ex: timing cannot run inside a graph capture");
+  JQC_REQUIRE(c->grad_tasks.valid || !capturing, JQC_ERR_NOT_READY,
               "jqc_grad2e: no gradient work list; call jqc_grad2e once before the capture");
+  JQC_REQUIRE(dens_tau <= 0.0 || !capturing || c->d_dmax.n >= (size_t)c->n_shell * c->n_shell, JQC_ERR_NOT_READY,
+              "jqc_grad2e: density screening scratch not allocated; call once before the capture");
   if (!c->grad_tasks.valid) {
     rc = build_tasks(c, c->grad_tasks, JQC_PREC_FP64, 0.0, false, s, true);
     if (rc) return rc;
   }
+  const float* dmax = nullptr;
+  if (dens_tau > 0.0) {
+    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
+    JQC_CUDA_CHECK(launch_dmax(D, n_dens, c->n_bf, c->n_shell, c->d_ao.ptr, c->d_l.ptr, c->d_dmax.ptr, s));
+    dmax = c->d_dmax.ptr;
+  }
+  const int n_pairs = (int)c->pairs.size();
+  JQC_REQUIRE(!capturing || c->d_pair_force.n >= (size_t)6 * n_pairs, JQC_ERR_NOT_READY,
+              "jqc_grad2e: force scratch not allocated; call jqc_grad2e once before the capture");
+  JQC_CUDA_CHECK(c->d_pair_force.reserve((size_t)6 * std::max(1, n_pairs)));
+  JQC_CUDA_CHECK(cudaMemsetAsync(c->d_pair_force.ptr, 0, (size_t)6 * n_pairs * sizeof(double), s));
+  if (class_ms)
+    for (int k = 0; k < kNumQuartetClasses; ++k) class_ms[k] = 0.0;
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
     GradParams p;
     p.tasks = c->grad_tasks.d.ptr + c->grad_tasks.off[0][qc];
@@ -951,13 +998,34 @@ int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k
     p.jscale = j_scale;
     p.kscale = k_scale;
     p.grad = grad;
+    p.pair_force = c->d_pair_force.ptr;
+    p.dmax = dmax;
+    p.n_shell = c->n_shell;
+    p.dens_tau = (float)dens_tau;
     const int pb = qc_bra(qc), pk = qc_ket(qc);
-    if (is_grad_reg_class(qc))
+    if (class_ms) JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));
+    const int ge = c->grad_engine[qc];
+    if (ge == kEngineReg)
       JQC_CUDA_CHECK(launch_grad_reg(qc, p, s));
+    else if (ge == kEngineCol)
+      JQC_CUDA_CHECK(launch_grad_row(qc, p, s));
     else
       JQC_CUDA_CHECK(launch_warp_grad(pc_la(pb), pc_lb(pb), pc_la(pk), pc_lb(pk), p, s));
+    if (class_ms) {
+      JQC_CUDA_CHECK(cudaEventRecord(c->ev_t1, s));
+      JQC_CUDA_CHECK(cudaEventSynchronize(c->ev_t1));
+      float ms = 0.f;
+      JQC_CUDA_CHECK(cudaEventElapsedTime(&ms, c->ev_t0, c->ev_t1));
+      class_ms[qc] = ms;
+    }
   }
+  JQC_CUDA_CHECK(launch_pair_force_reduce(c->d_pairs.ptr, n_pairs, c->d_atom.ptr, c->d_pair_force.ptr, grad, s));
   return JQC_OK;
+}
+
+int jqc_grad2e(jqc_ctx* c, int n_dens, const double* D, double j_scale, double k_scale, double* grad,
+               void* stream) {
+  return jqc_grad2e_ex(c, n_dens, D, j_scale, k_scale, 0.0, grad, stream, nullptr);
 }
 
 int jqc_grad1e(jqc_ctx* c, const double* D, const double* W, double* grad, void* stream) {
@@ -1118,9 +1186,10 @@ int jqc_graph_destroy(jqc_ctx* c, int graph_id) {
 int jqc_get_tuning(jqc_ctx* c, int* out) {
   JQC_REQUIRE(c && out, JQC_ERR_INVALID, "jqc_get_tuning: null argument");
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-    out[3 * qc] = c->tune[qc].threads;
-    out[3 * qc + 1] = c->tune[qc].lane_prims;
-    out[3 * qc + 2] = c->tune[qc].persistent;
+    out[kTuneInts * qc] = c->tune[qc].threads;
+    out[kTuneInts * qc + 1] = c->tune[qc].lane_prims;
+    out[kTuneInts * qc + 2] = c->tune[qc].persistent;
+    out[kTuneInts * qc + 3] = class_engine(c->tune[qc], qc);
   }
   return JQC_OK;
 }
@@ -1128,17 +1197,43 @@ int jqc_get_tuning(jqc_ctx* c, int* out) {
 int jqc_set_tuning(jqc_ctx* c, const int* cfg) {
   JQC_REQUIRE(c && cfg, JQC_ERR_INVALID, "jqc_set_tuning: null argument");
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-    const int th = cfg[3 * qc], lp = cfg[3 * qc + 1], pe = cfg[3 * qc + 2];
-    JQC_REQUIRE(th == 64 || th == 128 || th == 256, JQC_ERR_INVALID, "jqc_set_tuning: threads must be 64, 128 or 256");
-    JQC_REQUIRE(lp >= 1 && lp <= (1 << 20), JQC_ERR_INVALID, "jqc_set_tuning: lane_prims out of range");
-    JQC_REQUIRE(pe == 0 || pe == 1, JQC_ERR_INVALID, "jqc_set_tuning: persistent must be 0 or 1");
+    const int* q = cfg + kTuneInts * qc;
+    JQC_REQUIRE(q[0] == 64 || q[0] == 128 || q[0] == 256, JQC_ERR_INVALID,
+                "jqc_set_tuning: threads must be 64, 128 or 256");
+    JQC_REQUIRE(q[1] >= 1 && q[1] <= (1 << 20), JQC_ERR_INVALID, "jqc_set_tuning: lane_prims out of range");
+    JQC_REQUIRE(q[2] == 0 || q[2] == 1, JQC_ERR_INVALID, "jqc_set_tuning: persistent must be 0 or 1");
+    JQC_REQUIRE(engine_valid(q[3], qc), JQC_ERR_INVALID,
+                "jqc_set_tuning: engine must be 0 (register, L <= 6), 1 (column, L >= 5) or 2 (warp)");
   }
-  bool chunks_changed = false;
+  bool lists_changed = false;
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-    if (c->tune[qc].lane_prims != cfg[3 * qc + 1]) chunks_changed = true;
-    c->tune[qc] = ClassTune{cfg[3 * qc], cfg[3 * qc + 1], cfg[3 * qc + 2]};
+    const int* q = cfg + kTuneInts * qc;
+    const bool per_task_changed = (class_engine(c->tune[qc], qc) == kEngineReg) != (q[3] == kEngineReg);
+    if (c->tune[qc].lane_prims != q[1] || per_task_changed) lists_changed = true;
+    c->tune[qc] = ClassTune{q[0], q[1], q[2], q[3]};
   }
-  if (chunks_changed) drop_jk_tasks(c);  // the work lists depend on lane_prims
+  if (lists_changed) drop_jk_tasks(c);  // the work lists depend on lane_prims and the engine
+  return JQC_OK;
+}
+
+int jqc_set_grad_engine(jqc_ctx* c, int quartet_class, int engine) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_set_grad_engine: null context");
+  JQC_REQUIRE(quartet_class >= 0 && quartet_class < kNumQuartetClasses, JQC_ERR_INVALID,
+              "jqc_set_grad_engine: quartet class out of range");
+  JQC_REQUIRE(grad_engine_valid(engine, quartet_class), JQC_ERR_INVALID,
+              "jqc_set_grad_engine: engine must be 0 (register, L <= 4), 1 (row, dp/dd bra) or 2 (warp)");
+  const bool per_task_changed = (c->grad_engine[quartet_class] == kEngineReg) != (engine == kEngineReg);
+  c->grad_engine[quartet_class] = engine;
+  if (per_task_changed && c->grad_tasks.valid) {
+    drop_graphs(c);
+    c->grad_tasks.valid = false;
+  }
+  return JQC_OK;
+}
+
+int jqc_get_grad_engine(jqc_ctx* c, int* engines21) {
+  JQC_REQUIRE(c && engines21, JQC_ERR_INVALID, "jqc_get_grad_engine: null argument");
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) engines21[qc] = c->grad_engine[qc];
   return JQC_OK;
 }
 
@@ -1179,8 +1274,8 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
   rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
   if (rc) return rc;
   const std::string sig = tune_signature(c, c->jk_cur, n_dens, precision_mode, dens_tau);
-  int cfg[3 * kNumQuartetClasses];
-  // 1. cache hit: "signature<TAB>63 integers" per line
+  int cfg[kTuneInts * kNumQuartetClasses];
+  // 1. cache hit: "signature<TAB>84 integers" per line
   if (cache_path && cache_path[0]) {
     std::FILE* f = std::fopen(cache_path, "r");
     if (f) {
@@ -1195,13 +1290,13 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
           const char* q = line.c_str() + tab + 1;
           int k = 0;
           char* end = nullptr;
-          for (; k < 3 * kNumQuartetClasses; ++k) {
+          for (; k < kTuneInts * kNumQuartetClasses; ++k) {
             const long v = std::strtol(q, &end, 10);
             if (end == q) break;
             cfg[k] = (int)v;
             q = end;
           }
-          hit = (k == 3 * kNumQuartetClasses);
+          hit = (k == kTuneInts * kNumQuartetClasses);
         }
         if (ch == EOF) break;
       }
@@ -1236,28 +1331,49 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
   ClassTune best[kNumQuartetClasses];
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
     best[qc] = ClassTune{};
+    best[qc].engine = default_engine(qc);
     best_ms[qc] = 1e300;
   }
   double cur[kNumQuartetClasses];
-  // 2. block size and grid form (no work-list rebuild needed)
+  auto rebuild = [&]() -> int {
+    drop_jk_tasks(c);
+    return ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+  };
+  // 2. engine of every class (register / column / warp where available)
+  for (int e = kEngineReg; e <= kEngineWarp; ++e) {
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc)
+      c->tune[qc] = ClassTune{128, kMaxLanePrims, 0, engine_valid(e, qc) ? e : default_engine(qc)};
+    rc = rebuild();
+    if (rc) return rc;
+    rc = time_classes(cur);
+    if (rc) return rc;
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc)
+      if (engine_valid(e, qc) && cur[qc] < best_ms[qc]) {
+        best_ms[qc] = cur[qc];
+        best[qc].engine = e;
+      }
+  }
+  for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->tune[qc] = ClassTune{128, kMaxLanePrims, 0, best[qc].engine};
+  rc = rebuild();
+  if (rc) return rc;
+  // 3. block size and grid form of the register kernels (no rebuild needed)
   const int th_opts[3] = {64, 128, 256};
   for (int ti = 0; ti < 3; ++ti)
     for (int pe = 0; pe < 2; ++pe) {
       for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
         c->tune[qc].threads = th_opts[ti];
         c->tune[qc].persistent = pe;
-        c->tune[qc].lane_prims = kMaxLanePrims;
       }
       rc = time_classes(cur);
       if (rc) return rc;
       for (int qc = 0; qc < kNumQuartetClasses; ++qc)
-        if (cur[qc] < best_ms[qc]) {
+        if (best[qc].engine == kEngineReg && cur[qc] < best_ms[qc]) {
           best_ms[qc] = cur[qc];
           best[qc].threads = th_opts[ti];
           best[qc].persistent = pe;
         }
     }
-  // 3. bra primitive chunk (work list rebuilt per value)
+  // 4. bra primitive chunk (work list rebuilt per value)
   const int lp_opts[4] = {64, 128, 512, 1024};
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
     c->tune[qc].threads = best[qc].threads;
@@ -1265,8 +1381,7 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
   }
   for (int li = 0; li < 4; ++li) {
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->tune[qc].lane_prims = lp_opts[li];
-    drop_jk_tasks(c);
-    rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
+    rc = rebuild();
     if (rc) return rc;
     rc = time_classes(cur);
     if (rc) return rc;
@@ -1277,13 +1392,14 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
       }
   }
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-    if (!is_reg_class(qc)) {  // the warp engine has a fixed launch shape
+    if (best[qc].engine != kEngineReg) {  // the other engines have a fixed launch shape
       best[qc].threads = 128;
       best[qc].persistent = 0;
     }
-    cfg[3 * qc] = best[qc].threads;
-    cfg[3 * qc + 1] = best[qc].lane_prims;
-    cfg[3 * qc + 2] = best[qc].persistent;
+    cfg[kTuneInts * qc] = best[qc].threads;
+    cfg[kTuneInts * qc + 1] = best[qc].lane_prims;
+    cfg[kTuneInts * qc + 2] = best[qc].persistent;
+    cfg[kTuneInts * qc + 3] = best[qc].engine;
   }
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->tune[qc].lane_prims = -1;  // force a rebuild
   rc = jqc_set_tuning(c, cfg);
@@ -1294,7 +1410,7 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
     std::FILE* f = std::fopen(cache_path, "a");
     JQC_REQUIRE(f != nullptr, JQC_ERR_INVALID, "jqc_autotune: cannot open the cache file for appending");
     std::fprintf(f, "%s\t", sig.c_str());
-    for (int k = 0; k < 3 * kNumQuartetClasses; ++k) std::fprintf(f, k ? " %d" : "%d", cfg[k]);
+    for (int k = 0; k < kTuneInts * kNumQuartetClasses; ++k) std::fprintf(f, k ? " %d" : "%d", cfg[k]);
     std::fprintf(f, "\n");
     std::fclose(f);
   }

@@ -27,20 +27,42 @@
 
 namespace jqc {
 
-constexpr int kGMaxL = 9;                       // (dd|dd) + 1
-constexpr int kGMaxHerm = nherm(kGMaxL);        // 220
-constexpr int kGMaxX = 36 * nherm(5);           // ncd * nherm(LAB+1) <= 36 * 56
+constexpr int kGMaxL = 9;  // (dd|dd) + 1
+constexpr int kGradWarps = 4;  // warps per block of the warp-cooperative gradient
 
-struct GradSmem {
-  double R[kGMaxHerm];
-  double Rn[kGMaxL + 2];
-  double Eb[3][4][4][7];   // bra E, i <= la+1, j <= lb+1, t <= la+lb+2
-  double DA[3][3][3][6];   // derivative E on centre A, i <= la, j <= lb, t <= la+lb+1
-  double DB[3][3][3][6];
-  double Fk[3][4][3][6];   // ket E with (-1)^t, c <= lc+1, d <= ld
-  double DC[3][3][3][6];   // derivative ket E on centre C (signed)
-  double X[kGMaxX];
-  double G[36 * 36];       // Gamma_abcd
+// Shared-memory layout of one warp, sized for its class (la lb | lc ld):
+//   Eb[3][la+2][lb+2][la+lb+3]   bra E up to one order higher
+//   DA, DB[3][la+1][lb+1][la+lb+2] derivative E on the bra centres
+//   Fk[3][lc+2][ld+1][lc+ld+2]   ket E with (-1)^t
+//   DC[3][lc+1][ld+1][lc+ld+2]   derivative ket E on centre C
+//   Rn[L+2], R[nherm(L+1)], X[ncd * nherm(la+lb+1)], G[nab * ncd]
+struct GradLayout {
+  int ebJ, ebT, ebX, daJ, daT, daX, fkD, fkT, fkX, dcX;
+  int oDA, oDB, oFk, oDC, oRn, oR, oX, oG, total;
+  __host__ __device__ GradLayout(int la, int lb, int lc, int ld) {
+    ebJ = lb + 2;
+    ebT = la + lb + 3;
+    ebX = (la + 2) * ebJ * ebT;
+    daJ = lb + 1;
+    daT = la + lb + 2;
+    daX = (la + 1) * daJ * daT;
+    fkD = ld + 1;
+    fkT = lc + ld + 2;
+    fkX = (lc + 2) * fkD * fkT;
+    dcX = (lc + 1) * fkD * fkT;
+    const int L = la + lb + lc + ld;
+    const int ncd = ncart(lc) * ncart(ld), nab = ncart(la) * ncart(lb);
+    oDA = 3 * ebX;
+    oDB = oDA + 3 * daX;
+    oFk = oDB + 3 * daX;
+    oDC = oFk + 3 * fkX;
+    oRn = oDC + 3 * dcX;
+    oR = oRn + L + 2;
+    oX = oR + nherm(L + 1);
+    oG = oX + ncd * nherm(la + lb + 1);
+    total = oG + nab * ncd;
+    total = (total + 1) & ~1;  // keep every warp's slice 16-byte aligned
+  }
 };
 
 // E coefficients (runtime la, lb) along one axis into e[i][j][t] for
@@ -69,12 +91,32 @@ __device__ void gecoef(double (*e)[4][7], int la, int lb, double pa, double pb, 
       }
 }
 
-__global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int la, int lb, int lc, int ld) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  GradSmem* sm = reinterpret_cast<GradSmem*>(smraw);
+// One warp per task (a bra primitive range of one shell quartet, or of up to
+// nket quartets of one bra), kGradWarps warps per block, each with its own
+// slice of the dynamic shared memory.
+__global__ void __launch_bounds__(32 * kGradWarps, 4) warp_grad_kernel(const GradParams prm, int la, int lb, int lc,
+                                                                   int ld) {
+  extern __shared__ __align__(16) double smd[];
+  const GradLayout ly(la, lb, lc, ld);
   const int lane = threadIdx.x & 31;
-  const int task_id = blockIdx.x;
+  const int task_id = blockIdx.x * kGradWarps + (threadIdx.x >> 5);
   if (task_id >= prm.n_tasks) return;
+  double* base = smd + (size_t)(threadIdx.x >> 5) * ly.total;
+  double* const sEb = base;
+  double* const sDA = base + ly.oDA;
+  double* const sDB = base + ly.oDB;
+  double* const sFk = base + ly.oFk;
+  double* const sDC = base + ly.oDC;
+  double* const sRn = base + ly.oRn;
+  double* const sR = base + ly.oR;
+  double* const sX = base + ly.oX;
+  double* const sG = base + ly.oG;
+  auto EB = [&](int x, int i, int j, int t) -> double& { return sEb[x * ly.ebX + (i * ly.ebJ + j) * ly.ebT + t]; };
+  auto DA = [&](int x, int i, int j, int t) -> double& { return sDA[x * ly.daX + (i * ly.daJ + j) * ly.daT + t]; };
+  auto DB = [&](int x, int i, int j, int t) -> double& { return sDB[x * ly.daX + (i * ly.daJ + j) * ly.daT + t]; };
+  auto FK = [&](int x, int c, int d, int t) -> double& { return sFk[x * ly.fkX + (c * ly.fkD + d) * ly.fkT + t]; };
+  auto DC = [&](int x, int c, int d, int t) -> double& { return sDC[x * ly.dcX + (c * ly.fkD + d) * ly.fkT + t]; };
+
   const Task task = prm.tasks[task_id];
   const ShellPair bp = prm.pairs[task.bra];
   const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
@@ -93,6 +135,9 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
     const double Cx = ctr[3 * kp.a], Cy = ctr[3 * kp.a + 1], Cz = ctr[3 * kp.a + 2];
     const double Dx = ctr[3 * kp.b], Dy = ctr[3 * kp.b + 1], Dz = ctr[3 * kp.b + 2];
     const int c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];
+    // density screening (warp-uniform: one quartet at a time)
+    if (prm.dmax != nullptr && float(bp.Q) * float(kp.Q) * gamma_bound(prm, bp.a, bp.b, kp.a, kp.b) < prm.dens_tau)
+      continue;
     // Gamma for this quartet
     __syncwarp();
     for (int e = lane; e < ntot; e += 32) {
@@ -105,20 +150,24 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
         dcd += Ds[(size_t)ic * n + id];
         kx += Ds[(size_t)ia * n + ic] * Ds[(size_t)ib * n + id] + Ds[(size_t)ia * n + id] * Ds[(size_t)ib * n + ic];
       }
-      sm->G[e] = prm.jscale * dab * dcd - 0.5 * prm.kscale * kx;
+      sG[e] = prm.jscale * dab * dcd - 0.5 * prm.kscale * kx;
     }
     double g[9];
     for (int k = 0; k < 9; ++k) g[k] = 0.0;
 
-    for (int ip = 0; ip < bp.npp; ++ip) {
+    const int p0 = task.flags & 0xffff, p1 = task.flags >> 16;  // bra primitive-pair range
+    for (int ip = p0; ip < p1; ++ip) {
       const PrimPair bpp = prm.pp[bp.pp + ip];
       __syncwarp();
       if (lane < 3) {
         const double P = lane == 0 ? bpp.Px : lane == 1 ? bpp.Py : bpp.Pz;
         const double A = lane == 0 ? Ax : lane == 1 ? Ay : Az;
         const double B = lane == 0 ? Bx : lane == 1 ? By : Bz;
-        double(*E)[4][7] = sm->Eb[lane];
+        double E[4][4][7];
         gecoef(E, la + 1, lb + 1, P - A, P - B, bpp.h);
+        for (int i = 0; i <= la + 1; ++i)
+          for (int j = 0; j <= lb + 1; ++j)
+            for (int t = 0; t < ly.ebT; ++t) EB(lane, i, j, t) = E[i][j][t];
         for (int i = 0; i <= la; ++i)
           for (int j = 0; j <= lb; ++j)
             for (int t = 0; t <= la + lb + 1; ++t) {
@@ -126,8 +175,8 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
               if (i > 0) va -= i * E[i - 1][j][t];
               double vb = 2.0 * bpp.beta * E[i][j + 1][t];
               if (j > 0) vb -= j * E[i][j - 1][t];
-              sm->DA[lane][i][j][t] = va;
-              sm->DB[lane][i][j][t] = vb;
+              DA(lane, i, j, t) = va;
+              DB(lane, i, j, t) = vb;
             }
       }
       for (int iq = 0; iq < kp.npp; ++iq) {
@@ -137,18 +186,17 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
           const double Q = ax == 0 ? kpp.Px : ax == 1 ? kpp.Py : kpp.Pz;
           const double C = ax == 0 ? Cx : ax == 1 ? Cy : Cz;
           const double Dd = ax == 0 ? Dx : ax == 1 ? Dy : Dz;
-          double(*F)[3][6] = sm->Fk[ax];
           double tmp[4][4][7];
           gecoef(tmp, lc + 1, ld, Q - C, Q - Dd, kpp.h);
           for (int c = 0; c <= lc + 1; ++c)
             for (int d = 0; d <= ld; ++d)
-              for (int t = 0; t < 6; ++t) F[c][d][t] = (t & 1) ? -tmp[c][d][t] : tmp[c][d][t];
+              for (int t = 0; t < ly.fkT; ++t) FK(ax, c, d, t) = (t & 1) ? -tmp[c][d][t] : tmp[c][d][t];
           for (int c = 0; c <= lc; ++c)
             for (int d = 0; d <= ld; ++d)
-              for (int t = 0; t < 6; ++t) {
-                double v = 2.0 * kpp.alpha * F[c + 1][d][t];
-                if (c > 0) v -= c * F[c - 1][d][t];
-                sm->DC[ax][c][d][t] = v;
+              for (int t = 0; t < ly.fkT; ++t) {
+                double v = 2.0 * kpp.alpha * ((t & 1) ? -tmp[c + 1][d][t] : tmp[c + 1][d][t]);
+                if (c > 0) v -= c * ((t & 1) ? -tmp[c - 1][d][t] : tmp[c - 1][d][t]);
+                DC(ax, c, d, t) = v;
               }
         }
         // Boys and R up to L+1
@@ -160,33 +208,33 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
         if (lane <= L1) {
           double pref = 4.0 * kTwoPi25 * bpp.K * kpp.K * (bpp.h * kpp.h) * r;
           for (int k = 0; k < lane; ++k) pref *= -2.0 * rho;
-          sm->Rn[lane] = pref * boys_single<double>(tb, lane, prm.boys);
+          sRn[lane] = pref * boys_single<double>(tb, lane, prm.boys);
         }
         __syncwarp();
-        if (lane == 0) sm->R[0] = sm->Rn[L1];
+        if (lane == 0) sR[0] = sRn[L1];
         __syncwarp();
         for (int m = L1 - 1; m >= 0; --m) {
           for (int s = L1 - m; s >= 1; --s) {
-            const int base = s * (s + 1) * (s + 2) / 6;
+            const int base_s = s * (s + 1) * (s + 2) / 6;
             for (int k = lane; k < ncart(s); k += 32) {
               int t, u, v;
               wcart(s, k, t, u, v);
               double val;
               if (t > 0) {
-                val = X * sm->R[herm_index(t - 1, u, v)];
-                if (t > 1) val += (t - 1) * sm->R[herm_index(t - 2, u, v)];
+                val = X * sR[herm_index(t - 1, u, v)];
+                if (t > 1) val += (t - 1) * sR[herm_index(t - 2, u, v)];
               } else if (u > 0) {
-                val = Y * sm->R[herm_index(t, u - 1, v)];
-                if (u > 1) val += (u - 1) * sm->R[herm_index(t, u - 2, v)];
+                val = Y * sR[herm_index(t, u - 1, v)];
+                if (u > 1) val += (u - 1) * sR[herm_index(t, u - 2, v)];
               } else {
-                val = Z * sm->R[herm_index(t, u, v - 1)];
-                if (v > 1) val += (v - 1) * sm->R[herm_index(t, u, v - 2)];
+                val = Z * sR[herm_index(t, u, v - 1)];
+                if (v > 1) val += (v - 1) * sR[herm_index(t, u, v - 2)];
               }
-              sm->R[base + k] = val;
+              sR[base_s + k] = val;
             }
             __syncwarp();
           }
-          if (lane == 0) sm->R[0] = sm->Rn[m];
+          if (lane == 0) sR[0] = sRn[m];
           __syncwarp();
         }
         // stage 1: X[cd][h], h < nherm(lab+1)
@@ -199,47 +247,46 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
           double x = 0.0;
           for (int tp = 0; tp <= cx + dx; ++tp)
             for (int up = 0; up <= cy + dy; ++up) {
-              const double fxy = sm->Fk[0][cx][dx][tp] * sm->Fk[1][cy][dy][up];
-              for (int vp = 0; vp <= cz + dz; ++vp)
-                x += fxy * sm->Fk[2][cz][dz][vp] * sm->R[herm_index(t + tp, u + up, v + vp)];
+              const double fxy = FK(0, cx, dx, tp) * FK(1, cy, dy, up);
+              for (int vp = 0; vp <= cz + dz; ++vp) x += fxy * FK(2, cz, dz, vp) * sR[herm_index(t + tp, u + up, v + vp)];
             }
-          sm->X[idx] = x;
+          sX[idx] = x;
         }
         __syncwarp();
         // bra derivatives (A, B)
         for (int e = lane; e < ntot; e += 32) {
-          const double w = sm->G[e];
+          const double w = sG[e];
           if (w == 0.0) continue;
           const int ab = e / ncd, cd = e % ncd;
           int ax, ay, az, bx, by, bz;
           wcart(la, ab / nb, ax, ay, az);
           wcart(lb, ab % nb, bx, by, bz);
-          const double* Xc = sm->X + cd * nh1;
-          double s[6] = {0, 0, 0, 0, 0, 0};
+          const double* Xc = sX + cd * nh1;
+          double sacc[6] = {0, 0, 0, 0, 0, 0};
           for (int t = 0; t <= ax + bx + 1; ++t)
             for (int u = 0; u <= ay + by + 1; ++u)
               for (int v = 0; v <= az + bz + 1; ++v) {
-                const double xv = Xc[herm_index(t, u, v)];
-                const double ex = t <= ax + bx ? sm->Eb[0][ax][bx][t] : 0.0;
-                const double ey = u <= ay + by ? sm->Eb[1][ay][by][u] : 0.0;
-                const double ez = v <= az + bz ? sm->Eb[2][az][bz][v] : 0.0;
                 // exactly one axis may exceed its plain range
                 const int over = (t > ax + bx) + (u > ay + by) + (v > az + bz);
                 if (over > 1) continue;
+                const double xv = Xc[herm_index(t, u, v)];
+                const double ex = t <= ax + bx ? EB(0, ax, bx, t) : 0.0;
+                const double ey = u <= ay + by ? EB(1, ay, by, u) : 0.0;
+                const double ez = v <= az + bz ? EB(2, az, bz, v) : 0.0;
                 if (u <= ay + by && v <= az + bz) {
-                  s[0] += sm->DA[0][ax][bx][t] * ey * ez * xv;
-                  s[3] += sm->DB[0][ax][bx][t] * ey * ez * xv;
+                  sacc[0] += DA(0, ax, bx, t) * ey * ez * xv;
+                  sacc[3] += DB(0, ax, bx, t) * ey * ez * xv;
                 }
                 if (t <= ax + bx && v <= az + bz) {
-                  s[1] += ex * sm->DA[1][ay][by][u] * ez * xv;
-                  s[4] += ex * sm->DB[1][ay][by][u] * ez * xv;
+                  sacc[1] += ex * DA(1, ay, by, u) * ez * xv;
+                  sacc[4] += ex * DB(1, ay, by, u) * ez * xv;
                 }
                 if (t <= ax + bx && u <= ay + by) {
-                  s[2] += ex * ey * sm->DA[2][az][bz][v] * xv;
-                  s[5] += ex * ey * sm->DB[2][az][bz][v] * xv;
+                  sacc[2] += ex * ey * DA(2, az, bz, v) * xv;
+                  sacc[5] += ex * ey * DB(2, az, bz, v) * xv;
                 }
               }
-          for (int k = 0; k < 6; ++k) g[k] += w * s[k];
+          for (int k = 0; k < 6; ++k) g[k] += w * sacc[k];
         }
         // ket derivative (C), one axis at a time
         for (int dir = 0; dir < 3; ++dir) {
@@ -255,29 +302,29 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
             for (int tp = 0; tp <= tx; ++tp)
               for (int up = 0; up <= ty; ++up)
                 for (int vp = 0; vp <= tz; ++vp) {
-                  const double fx = dir == 0 ? sm->DC[0][cx][dx][tp] : (tp <= cx + dx ? sm->Fk[0][cx][dx][tp] : 0.0);
-                  const double fy = dir == 1 ? sm->DC[1][cy][dy][up] : (up <= cy + dy ? sm->Fk[1][cy][dy][up] : 0.0);
-                  const double fz = dir == 2 ? sm->DC[2][cz][dz][vp] : (vp <= cz + dz ? sm->Fk[2][cz][dz][vp] : 0.0);
-                  x += fx * fy * fz * sm->R[herm_index(t + tp, u + up, v + vp)];
+                  const double fx = dir == 0 ? DC(0, cx, dx, tp) : (tp <= cx + dx ? FK(0, cx, dx, tp) : 0.0);
+                  const double fy = dir == 1 ? DC(1, cy, dy, up) : (up <= cy + dy ? FK(1, cy, dy, up) : 0.0);
+                  const double fz = dir == 2 ? DC(2, cz, dz, vp) : (vp <= cz + dz ? FK(2, cz, dz, vp) : 0.0);
+                  x += fx * fy * fz * sR[herm_index(t + tp, u + up, v + vp)];
                 }
-            sm->X[idx] = x;
+            sX[idx] = x;
           }
           __syncwarp();
           for (int e = lane; e < ntot; e += 32) {
-            const double w = sm->G[e];
+            const double w = sG[e];
             if (w == 0.0) continue;
             const int ab = e / ncd, cd = e % ncd;
             int ax, ay, az, bx, by, bz;
             wcart(la, ab / nb, ax, ay, az);
             wcart(lb, ab % nb, bx, by, bz);
-            const double* Xc = sm->X + cd * nh0;
-            double s = 0.0;
+            const double* Xc = sX + cd * nh0;
+            double sacc = 0.0;
             for (int t = 0; t <= ax + bx; ++t)
               for (int u = 0; u <= ay + by; ++u) {
-                const double exy = sm->Eb[0][ax][bx][t] * sm->Eb[1][ay][by][u];
-                for (int v = 0; v <= az + bz; ++v) s += exy * sm->Eb[2][az][bz][v] * Xc[herm_index(t, u, v)];
+                const double exy = EB(0, ax, bx, t) * EB(1, ay, by, u);
+                for (int v = 0; v <= az + bz; ++v) sacc += exy * EB(2, az, bz, v) * Xc[herm_index(t, u, v)];
               }
-            g[6 + dir] += w * s;
+            g[6 + dir] += w * sacc;
           }
         }
         __syncwarp();
@@ -296,23 +343,51 @@ __global__ void __launch_bounds__(32) warp_grad_kernel(const GradParams prm, int
       g[k] = v * sc;
     }
     if (lane == 0) {
-      double* gr = prm.grad;
-      const int at[3] = {prm.atom[bp.a], prm.atom[bp.b], prm.atom[kp.a]};
-      const int atD = prm.atom[kp.b];
+      double* pf = prm.pair_force;
+      for (int k = 0; k < 6; ++k) atomicAdd(pf + 6 * task.bra + k, g[k]);
       for (int k = 0; k < 3; ++k) {
-        for (int c = 0; c < 3; ++c) atomicAdd(gr + 3 * at[c] + k, g[3 * c + k]);
-        atomicAdd(gr + 3 * atD + k, -(g[k] + g[3 + k] + g[6 + k]));
+        atomicAdd(pf + 6 * kidx + k, g[6 + k]);
+        atomicAdd(pf + 6 * kidx + 3 + k, -(g[k] + g[3 + k] + g[6 + k]));
       }
     }
   }
 }
 
+// Fold the per-shell-pair forces into the atoms: one thread per pair.
+__global__ void pair_force_reduce_kernel(const ShellPair* pairs, int n_pairs, const int* atom,
+                                         const double* pair_force, double* grad) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_pairs) return;
+  const ShellPair sp = pairs[p];
+  const int ta = atom[sp.a], tb = atom[sp.b];
+  const double* f = pair_force + 6 * (size_t)p;
+  for (int k = 0; k < 3; ++k) {
+    if (f[k] != 0.0) atomicAdd(grad + 3 * ta + k, f[k]);
+    if (f[3 + k] != 0.0) atomicAdd(grad + 3 * tb + k, f[3 + k]);
+  }
+}
+
+cudaError_t launch_pair_force_reduce(const ShellPair* pairs, int n_pairs, const int* atom, const double* pair_force,
+                                     double* grad, cudaStream_t s) {
+  if (n_pairs <= 0) return cudaSuccess;
+  pair_force_reduce_kernel<<<(n_pairs + 255) / 256, 256, 0, s>>>(pairs, n_pairs, atom, pair_force, grad);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_warp_grad(int la, int lb, int lc, int ld, const GradParams& p, cudaStream_t s) {
   if (p.n_tasks == 0) return cudaSuccess;
-  const size_t sm = sizeof(GradSmem);
-  cudaError_t e = cudaFuncSetAttribute(warp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  warp_grad_kernel<<<p.n_tasks, 32, sm, s>>>(p, la, lb, lc, ld);
+  const GradLayout ly(la, lb, lc, ld);
+  const size_t sm = (size_t)kGradWarps * ly.total * sizeof(double);
+  static size_t configured = 0;
+  if (sm > configured) {
+    // the largest class, (dd|dd), needs 4 x 36 KB
+    cudaError_t e = cudaFuncSetAttribute(warp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kGradWarps * GradLayout(2, 2, 2, 2).total * sizeof(double)));
+    if (e != cudaSuccess) return e;
+    configured = (size_t)kGradWarps * GradLayout(2, 2, 2, 2).total * sizeof(double);
+  }
+  const unsigned grid = (unsigned)((p.n_tasks + kGradWarps - 1) / kGradWarps);
+  warp_grad_kernel<<<grid, 32 * kGradWarps, sm, s>>>(p, la, lb, lc, ld);
   return cudaGetLastError();
 }
 

@@ -59,9 +59,14 @@ struct GradBody {
 
     const Task task = prm.tasks[warp];
     const ShellPair bp = prm.pairs[task.bra];
-    const bool active = lane < task.nket;
-    const int kidx = task.ket0 + (active ? lane : 0);
+    const bool in_range = lane < task.nket;
+    const int kidx = task.ket0 + (in_range ? lane : 0);
     const ShellPair kp = prm.pairs[kidx];
+    bool active = in_range;
+    if (prm.dmax != nullptr && active &&
+        float(bp.Q) * float(kp.Q) * gamma_bound(prm, bp.a, bp.b, kp.a, kp.b) < prm.dens_tau)
+      active = false;
+    if (__ballot_sync(0xffffffffu, active) == 0u) return;
     const double* ctr = prm.centres;
     const Vec3<double> A{ctr[3 * bp.a], ctr[3 * bp.a + 1], ctr[3 * bp.a + 2]};
     const Vec3<double> B{ctr[3 * bp.b], ctr[3 * bp.b + 1], ctr[3 * bp.b + 2]};
@@ -92,7 +97,8 @@ struct GradBody {
     static_for<9>([&](auto k) { g[decltype(k)::value] = 0.0; });
     const int nket = active ? kp.npp : 0;
 
-    for (int ip = 0; ip < bp.npp; ++ip) {
+    const int p0 = task.flags & 0xffff, p1 = task.flags >> 16;  // bra primitive-pair range
+    for (int ip = p0; ip < p1; ++ip) {
       const PrimPair bpp = prm.pp[bp.pp + ip];
       __syncwarp();
       if (lane < 3) {
@@ -269,19 +275,17 @@ struct GradBody {
     if (kp.diag) sc *= 0.5;
     if (task.bra == kidx) sc *= 0.5;
     static_for<9>([&](auto k) { g[decltype(k)::value] *= sc; });
-    double* gr = prm.grad;
-    const int atA = prm.atom[bp.a], atB = prm.atom[bp.b];
+    double* pf = prm.pair_force;
     static_for<6>([&](auto k_) {
       constexpr int k = decltype(k_)::value;
       const double v = warp_sum(g[k]);
-      if (lane == 0) atomicAdd(gr + 3 * (k < 3 ? atA : atB) + k % 3, v);
+      if (lane == 0) atomicAdd(pf + 6 * task.bra + k, v);
     });
     if (active) {
-      const int atC = prm.atom[kp.a], atD = prm.atom[kp.b];
       static_for<3>([&](auto k_) {
         constexpr int k = decltype(k_)::value;
-        atomicAdd(gr + 3 * atC + k, g[6 + k]);
-        atomicAdd(gr + 3 * atD + k, -(g[k] + g[3 + k] + g[6 + k]));
+        atomicAdd(pf + 6 * kidx + k, g[6 + k]);
+        atomicAdd(pf + 6 * kidx + 3 + k, -(g[k] + g[3 + k] + g[6 + k]));
       });
     }
   }

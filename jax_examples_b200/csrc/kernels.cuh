@@ -13,6 +13,11 @@ __host__ __device__ constexpr int pair_class(int la, int lb) {  // la >= lb
 }
 __host__ __device__ constexpr int quartet_class(int pb, int pk) { return pb * (pb + 1) / 2 + pk; }
 
+// Engines that can evaluate a J/K class: the register kernels (lane = ket
+// pair, L <= 6), the column engine (compile-time class, lane = ket Cartesian
+// pair, L >= 5) and the runtime-class warp engine (every class).
+enum JKEngine { kEngineReg = 0, kEngineCol = 1, kEngineWarp = 2 };
+
 struct JKParams {
   const Task* tasks;
   int n_tasks;
@@ -32,6 +37,7 @@ struct JKParams {
   float dens_tau;
   int threads = 128;       // threads per block (64, 128, 256)
   int persistent = 0;      // 1: grid capped at the resident blocks, warps stride over tasks
+  int engine = kEngineReg; // JKEngine
 };
 
 constexpr int kMaxJKThreads = 256;
@@ -110,7 +116,25 @@ struct GradParams {
   int n;
   double jscale, kscale;
   double* grad;           // n_atom x 3 (accumulated)
+  // Per-shell-pair force slots, 6 per pair (centre a xyz, centre b xyz):
+  // the kernels add into these (few collisions) and launch_pair_force_reduce
+  // folds them into grad (n_atom x 3 would take every atomic of the launch).
+  double* pair_force = nullptr;
+  const float* dmax = nullptr;  // n_shell x n_shell max |D^s| per shell block, or null
+  int n_shell = 0;
+  float dens_tau = 0.f;   // skip quartets whose Gamma bound x Q_ab Q_cd is below this
 };
+
+// Upper bound of |Gamma_abcd| over a shell quartet from the per-block density
+// maxima m (max over the n_dens densities): |D^t| <= n_dens m, so
+// |Gamma| <= j n_dens^2 m_ab m_cd + (k/2) n_dens (m_ac m_bd + m_ad m_bc).
+__device__ __forceinline__ float gamma_bound(const GradParams& p, int a, int b, int c, int d) {
+  const float* m = p.dmax;
+  const int ns = p.n_shell;
+  const float nd = float(p.n_dens);
+  return float(p.jscale) * nd * nd * m[a * ns + b] * m[c * ns + d] +
+         0.5f * float(p.kscale) * nd * (m[a * ns + c] * m[b * ns + d] + m[a * ns + d] * m[b * ns + c]);
+}
 
 struct Grad1Params {
   int n_shell, n, n_atom;
@@ -136,10 +160,17 @@ struct Grad1Params {
 // the warp-cooperative gradient kernel.
 __host__ __device__ constexpr bool is_grad_reg_class(int qc) { return qc_L(qc) <= 4; }
 cudaError_t launch_grad_reg(int qc, const GradParams& p, cudaStream_t s);
+bool has_grad_row_class(int qc);
+cudaError_t launch_grad_row(int qc, const GradParams& p, cudaStream_t s);
 cudaError_t launch_warp_grad(int la, int lb, int lc, int ld, const GradParams& p, cudaStream_t s);
 cudaError_t launch_grad1e(const Grad1Params& p, cudaStream_t s);
+cudaError_t launch_pair_force_reduce(const ShellPair* pairs, int n_pairs, const int* atom, const double* pair_force,
+                                     double* grad, cudaStream_t s);
 
 cudaError_t launch_warp_jk(int la, int lb, int lc, int ld, bool fp32, const JKParams& p, cudaStream_t s);
+bool has_col_class(int qc);
+cudaError_t launch_col_jk(int qc, bool fp32, const JKParams& p, cudaStream_t s);
+
 cudaError_t launch_warp_tensor(int la, int lb, int lc, int ld, const TensorParams& p, cudaStream_t s);
 cudaError_t launch_warp_schwarz(int la, int lb, const SchwarzParams& p, cudaStream_t s);
 cudaError_t launch_warp_prim(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s);

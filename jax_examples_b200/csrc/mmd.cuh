@@ -196,6 +196,10 @@ __device__ __forceinline__ void prim_quartet_R(const PPT& bp, const PPT& kp, con
   hermite_R<T, L>(R, Rn, PQx, PQy, PQz);
 }
 
+// Classes whose bra angular sum is at most this loop over ket primitives
+// outermost (see quartet_accumulate).
+constexpr int kKetOuterMaxLab = 1;
+
 // Accumulates the contracted block (ab|cd) for the ket Cartesian pairs of
 // part PART into out[ab][cdi] (cd = CD0 + cdi).  Loops over all primitive
 // pairs of the bra (outer) and ket (inner) shell pairs.  The bra E
@@ -217,86 +221,112 @@ __device__ __forceinline__ void quartet_accumulate(
     static_for<Cfg::CDP>([&](auto c) { out[decltype(ab)::value][decltype(c)::value] = T(0); });
   });
   if constexpr (Cfg::NCDP > 0) {
-    const int lane = threadIdx.x & 31;
-    for (int ip = 0; ip < nbra; ++ip) {
-      typename PPType<T>::type bp;
-      if constexpr (GLOBAL_PP) bp = ld_pp(bra + ip);
-      else bp = bra[ip];
-      const T inv2p = bp.h;
-      if constexpr (SHARED_BRA) {
-        __syncwarp();
-        if (lane == 0) ecoef_compute<T, LA, LB, false>(ebra[0], bp.Px - A.x, bp.Px - B.x, inv2p);
-        if (lane == 1) ecoef_compute<T, LA, LB, false>(ebra[1], bp.Py - A.y, bp.Py - B.y, inv2p);
-        if (lane == 2) ecoef_compute<T, LA, LB, false>(ebra[2], bp.Pz - A.z, bp.Pz - B.z, inv2p);
-        __syncwarp();
-      } else {
-        ecoef_compute<T, LA, LB, false>(ebra[0], bp.Px - A.x, bp.Px - B.x, inv2p);
-        ecoef_compute<T, LA, LB, false>(ebra[1], bp.Py - A.y, bp.Py - B.y, inv2p);
-        ecoef_compute<T, LA, LB, false>(ebra[2], bp.Pz - A.z, bp.Pz - B.z, inv2p);
-      }
-      const EArr<T, LA, LB> Ex = ebra[0], Ey = ebra[1], Ez = ebra[2];
-      for (int iq = 0; iq < nket; ++iq) {
-        typename PPType<T>::type kp;
-        if constexpr (GLOBAL_PP) kp = ld_pp(ket + iq);
-        else kp = ket[iq];
-        const T inv2q = kp.h;
-        T fbuf[3][LC + 1][LD + 1][LC + LD + 1];
-        ecoef_compute<T, LC, LD, true>(fbuf[0], kp.Px - C.x, kp.Px - D.x, inv2q);
-        ecoef_compute<T, LC, LD, true>(fbuf[1], kp.Py - C.y, kp.Py - D.y, inv2q);
-        ecoef_compute<T, LC, LD, true>(fbuf[2], kp.Pz - C.z, kp.Pz - D.z, inv2q);
-        const EArr<T, LC, LD> Fx = fbuf[0], Fy = fbuf[1], Fz = fbuf[2];
-        T R[nherm(L)];
-        prim_quartet_R<T, L>(bp, kp, boys_tab, R);
-
-        static_for<Cfg::NCDP>([&](auto cdi_) {
-          constexpr int cdi = decltype(cdi_)::value;
-          constexpr int cd = Cfg::CD0 + cdi, c = cd / Cfg::ND, d = cd % Cfg::ND;
-          constexpr int cx = cart_lx(LC, c), cy = cart_ly(LC, c), cz = cart_lz(LC, c);
-          constexpr int dx = cart_lx(LD, d), dy = cart_ly(LD, d), dz = cart_lz(LD, d);
-          // stage 1: X_tuv = sum_{t'u'v'} F^x F^y F^z R_{t+t',u+u',v+v'}
-          T X[nherm(LAB)];
-          static_for<nherm(LAB)>([&](auto h) { X[decltype(h)::value] = T(0); });
-          static_for<cx + dx + 1>([&](auto tp_) {
-            constexpr int tp = decltype(tp_)::value;
-            static_for<cy + dy + 1>([&](auto up_) {
-              constexpr int up = decltype(up_)::value;
-              const T fxy = Fx[cx][dx][tp] * Fy[cy][dy][up];
-              static_for<cz + dz + 1>([&](auto vp_) {
-                constexpr int vp = decltype(vp_)::value;
-                const T f = fxy * Fz[cz][dz][vp];
-                static_for<nherm(LAB)>([&](auto h_) {
-                  constexpr int h = decltype(h_)::value;
-                  constexpr int s = (h >= 20) ? 4 : (h >= 10) ? 3 : (h >= 4) ? 2 : (h >= 1) ? 1 : 0;
-                  constexpr int k = h - s * (s + 1) * (s + 2) / 6;
-                  constexpr int t = cart_lx(s, k), u = cart_ly(s, k), v = s - t - u;
-                  X[h] += f * R[herm_index(t + tp, u + up, v + vp)];
-                });
+    using PPT = typename PPType<T>::type;
+    // One primitive quartet: R, stage 1 (ket E against R) and stage 2 (bra E).
+    auto prim = [&](const PPT& bp, const EArr<T, LA, LB> Ex, const EArr<T, LA, LB> Ey, const EArr<T, LA, LB> Ez,
+                    const PPT& kp, const EArr<T, LC, LD> Fx, const EArr<T, LC, LD> Fy, const EArr<T, LC, LD> Fz) {
+      T R[nherm(L)];
+      prim_quartet_R<T, L>(bp, kp, boys_tab, R);
+      static_for<Cfg::NCDP>([&](auto cdi_) {
+        constexpr int cdi = decltype(cdi_)::value;
+        constexpr int cd = Cfg::CD0 + cdi, c = cd / Cfg::ND, d = cd % Cfg::ND;
+        constexpr int cx = cart_lx(LC, c), cy = cart_ly(LC, c), cz = cart_lz(LC, c);
+        constexpr int dx = cart_lx(LD, d), dy = cart_ly(LD, d), dz = cart_lz(LD, d);
+        // stage 1: X_tuv = sum_{t'u'v'} F^x F^y F^z R_{t+t',u+u',v+v'}
+        T X[nherm(LAB)];
+        static_for<nherm(LAB)>([&](auto h) { X[decltype(h)::value] = T(0); });
+        static_for<cx + dx + 1>([&](auto tp_) {
+          constexpr int tp = decltype(tp_)::value;
+          static_for<cy + dy + 1>([&](auto up_) {
+            constexpr int up = decltype(up_)::value;
+            const T fxy = Fx[cx][dx][tp] * Fy[cy][dy][up];
+            static_for<cz + dz + 1>([&](auto vp_) {
+              constexpr int vp = decltype(vp_)::value;
+              const T f = fxy * Fz[cz][dz][vp];
+              static_for<nherm(LAB)>([&](auto h_) {
+                constexpr int h = decltype(h_)::value;
+                constexpr int s = (h >= 20) ? 4 : (h >= 10) ? 3 : (h >= 4) ? 2 : (h >= 1) ? 1 : 0;
+                constexpr int k = h - s * (s + 1) * (s + 2) / 6;
+                constexpr int t = cart_lx(s, k), u = cart_ly(s, k), v = s - t - u;
+                X[h] += f * R[herm_index(t + tp, u + up, v + vp)];
               });
-            });
-          });
-          // stage 2: out[ab][cd] += sum_tuv E^x E^y E^z X_tuv
-          static_for<Cfg::NA>([&](auto a_) {
-            constexpr int a = decltype(a_)::value;
-            constexpr int ax = cart_lx(LA, a), ay = cart_ly(LA, a), az = cart_lz(LA, a);
-            static_for<Cfg::NB>([&](auto b_) {
-              constexpr int b = decltype(b_)::value;
-              constexpr int bx = cart_lx(LB, b), by = cart_ly(LB, b), bz = cart_lz(LB, b);
-              T acc = T(0);
-              static_for<ax + bx + 1>([&](auto t_) {
-                constexpr int t = decltype(t_)::value;
-                static_for<ay + by + 1>([&](auto u_) {
-                  constexpr int u = decltype(u_)::value;
-                  const T exy = Ex[ax][bx][t] * Ey[ay][by][u];
-                  static_for<az + bz + 1>([&](auto v_) {
-                    constexpr int v = decltype(v_)::value;
-                    acc += exy * Ez[az][bz][v] * X[herm_index(t, u, v)];
-                  });
-                });
-              });
-              out[a * Cfg::NB + b][cdi] += acc;
             });
           });
         });
+        // stage 2: out[ab][cd] += sum_tuv E^x E^y E^z X_tuv
+        static_for<Cfg::NA>([&](auto a_) {
+          constexpr int a = decltype(a_)::value;
+          constexpr int ax = cart_lx(LA, a), ay = cart_ly(LA, a), az = cart_lz(LA, a);
+          static_for<Cfg::NB>([&](auto b_) {
+            constexpr int b = decltype(b_)::value;
+            constexpr int bx = cart_lx(LB, b), by = cart_ly(LB, b), bz = cart_lz(LB, b);
+            T acc = T(0);
+            static_for<ax + bx + 1>([&](auto t_) {
+              constexpr int t = decltype(t_)::value;
+              static_for<ay + by + 1>([&](auto u_) {
+                constexpr int u = decltype(u_)::value;
+                const T exy = Ex[ax][bx][t] * Ey[ay][by][u];
+                static_for<az + bz + 1>([&](auto v_) {
+                  constexpr int v = decltype(v_)::value;
+                  acc += exy * Ez[az][bz][v] * X[herm_index(t, u, v)];
+                });
+              });
+            });
+            out[a * Cfg::NB + b][cdi] += acc;
+          });
+        });
+      });
+    };
+    auto ket_e = [&](const PPT& kp, T (*fbuf)[LC + 1][LD + 1][LC + LD + 1]) {
+      ecoef_compute<T, LC, LD, true>(fbuf[0], kp.Px - C.x, kp.Px - D.x, kp.h);
+      ecoef_compute<T, LC, LD, true>(fbuf[1], kp.Py - C.y, kp.Py - D.y, kp.h);
+      ecoef_compute<T, LC, LD, true>(fbuf[2], kp.Pz - C.z, kp.Pz - D.z, kp.h);
+    };
+    if constexpr (GLOBAL_PP && LA + LB <= kKetOuterMaxLab) {
+      // Ket primitives outer: each lane reads its ket primitive pair and its
+      // E coefficients once; the bra primitive pairs (the same address in
+      // every lane: one broadcast read) and their few E coefficients are
+      // redone per ket primitive in registers.  Cuts the per-lane global
+      // reads of the low-L classes, which are bound by L1 throughput.
+      for (int iq = 0; iq < nket; ++iq) {
+        const PPT kp = ld_pp(ket + iq);
+        T fbuf[3][LC + 1][LD + 1][LC + LD + 1];
+        ket_e(kp, fbuf);
+        for (int ip = 0; ip < nbra; ++ip) {
+          const PPT bp = ld_pp(bra + ip);
+          T eb[3][LA + 1][LB + 1][LA + LB + 1];
+          ecoef_compute<T, LA, LB, false>(eb[0], bp.Px - A.x, bp.Px - B.x, bp.h);
+          ecoef_compute<T, LA, LB, false>(eb[1], bp.Py - A.y, bp.Py - B.y, bp.h);
+          ecoef_compute<T, LA, LB, false>(eb[2], bp.Pz - A.z, bp.Pz - B.z, bp.h);
+          prim(bp, eb[0], eb[1], eb[2], kp, fbuf[0], fbuf[1], fbuf[2]);
+        }
+      }
+    } else {
+      const int lane = threadIdx.x & 31;
+      for (int ip = 0; ip < nbra; ++ip) {
+        PPT bp;
+        if constexpr (GLOBAL_PP) bp = ld_pp(bra + ip);
+        else bp = bra[ip];
+        const T inv2p = bp.h;
+        if constexpr (SHARED_BRA) {
+          __syncwarp();
+          if (lane == 0) ecoef_compute<T, LA, LB, false>(ebra[0], bp.Px - A.x, bp.Px - B.x, inv2p);
+          if (lane == 1) ecoef_compute<T, LA, LB, false>(ebra[1], bp.Py - A.y, bp.Py - B.y, inv2p);
+          if (lane == 2) ecoef_compute<T, LA, LB, false>(ebra[2], bp.Pz - A.z, bp.Pz - B.z, inv2p);
+          __syncwarp();
+        } else {
+          ecoef_compute<T, LA, LB, false>(ebra[0], bp.Px - A.x, bp.Px - B.x, inv2p);
+          ecoef_compute<T, LA, LB, false>(ebra[1], bp.Py - A.y, bp.Py - B.y, inv2p);
+          ecoef_compute<T, LA, LB, false>(ebra[2], bp.Pz - A.z, bp.Pz - B.z, inv2p);
+        }
+        for (int iq = 0; iq < nket; ++iq) {
+          PPT kp;
+          if constexpr (GLOBAL_PP) kp = ld_pp(ket + iq);
+          else kp = ket[iq];
+          T fbuf[3][LC + 1][LD + 1][LC + LD + 1];
+          ket_e(kp, fbuf);
+          prim(bp, ebra[0], ebra[1], ebra[2], kp, fbuf[0], fbuf[1], fbuf[2]);
+        }
       }
     }
   }

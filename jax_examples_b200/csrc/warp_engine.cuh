@@ -249,4 +249,66 @@ struct WarpQuartet {
   }
 };
 
+// J/K digestion of one finished contracted block blk[ab * ncd + cd] (shared
+// memory, all lanes call) with scale s: J[a][b] and J[c][d] (Coulomb of both
+// pairs) and the four exchange blocks K[a][d], K[a][c], K[b][d], K[b][c],
+// lanes spread over output elements, one atomic per element.
+template <typename T>
+__device__ __forceinline__ void warp_digest_jk(const JKParams& prm, const T* blk, int na, int nb, int nc, int nd,
+                                               int a0, int b0, int c0, int d0, double s, int lane) {
+  const int n = prm.n;
+  const int ncd = nc * nd;
+  for (int dd = 0; dd < prm.n_dens; ++dd) {
+    const double* Dm = prm.D + (size_t)dd * n * n;
+    double* Jm = prm.J + (size_t)dd * n * n;
+    double* Km = prm.K + (size_t)dd * n * n;
+    for (int ab = lane; ab < na * nb; ab += 32) {
+      double acc = 0.0;
+      for (int cd = 0; cd < ncd; ++cd)
+        acc += double(blk[ab * ncd + cd]) * __ldg(Dm + (size_t)(c0 + cd / nd) * n + d0 + cd % nd);
+      atomicAdd(Jm + (size_t)(a0 + ab / nb) * n + b0 + ab % nb, 2.0 * s * acc);
+    }
+    for (int cd = lane; cd < ncd; cd += 32) {
+      double acc = 0.0;
+      for (int ab = 0; ab < na * nb; ++ab)
+        acc += double(blk[ab * ncd + cd]) * __ldg(Dm + (size_t)(a0 + ab / nb) * n + b0 + ab % nb);
+      atomicAdd(Jm + (size_t)(c0 + cd / nd) * n + d0 + cd % nd, 2.0 * s * acc);
+    }
+    // K[a][d] += v D[c][b]; K[a][c] += v D[d][b]
+    for (int idx = lane; idx < na * (nd + nc); idx += 32) {
+      const int a = idx / (nd + nc), r = idx % (nd + nc);
+      double acc = 0.0;
+      if (r < nd) {
+        for (int b = 0; b < nb; ++b)
+          for (int c = 0; c < nc; ++c)
+            acc += double(blk[(a * nb + b) * ncd + c * nd + r]) * __ldg(Dm + (size_t)(c0 + c) * n + b0 + b);
+        atomicAdd(Km + (size_t)(a0 + a) * n + d0 + r, s * acc);
+      } else {
+        const int c = r - nd;
+        for (int b = 0; b < nb; ++b)
+          for (int d = 0; d < nd; ++d)
+            acc += double(blk[(a * nb + b) * ncd + c * nd + d]) * __ldg(Dm + (size_t)(d0 + d) * n + b0 + b);
+        atomicAdd(Km + (size_t)(a0 + a) * n + c0 + c, s * acc);
+      }
+    }
+    // K[b][d] += v D[c][a]; K[b][c] += v D[d][a]
+    for (int idx = lane; idx < nb * (nd + nc); idx += 32) {
+      const int b = idx / (nd + nc), r = idx % (nd + nc);
+      double acc = 0.0;
+      if (r < nd) {
+        for (int a = 0; a < na; ++a)
+          for (int c = 0; c < nc; ++c)
+            acc += double(blk[(a * nb + b) * ncd + c * nd + r]) * __ldg(Dm + (size_t)(c0 + c) * n + a0 + a);
+        atomicAdd(Km + (size_t)(b0 + b) * n + d0 + r, s * acc);
+      } else {
+        const int c = r - nd;
+        for (int a = 0; a < na; ++a)
+          for (int d = 0; d < nd; ++d)
+            acc += double(blk[(a * nb + b) * ncd + c * nd + d]) * __ldg(Dm + (size_t)(d0 + d) * n + a0 + a);
+        atomicAdd(Km + (size_t)(b0 + b) * n + c0 + c, s * acc);
+      }
+    }
+  }
+}
+
 }  // namespace jqc

@@ -68,60 +68,7 @@ __global__ void __launch_bounds__(kWarpBlock) warp_jk_kernel(const JKParams prm,
     if (bp.diag) s *= 0.5;
     if (kp.diag) s *= 0.5;
     if (task.bra == kidx) s *= 0.5;
-    const int a0 = prm.ao[bp.a], b0 = prm.ao[bp.b], c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];
-    const int ncd = nc * nd;
-    const T* blk = sm->XB;
-    for (int dd = 0; dd < prm.n_dens; ++dd) {
-      const double* Dm = prm.D + (size_t)dd * n * n;
-      double* Jm = prm.J + (size_t)dd * n * n;
-      double* Km = prm.K + (size_t)dd * n * n;
-      for (int ab = lane; ab < na * nb; ab += 32) {
-        double acc = 0.0;
-        for (int cd = 0; cd < ncd; ++cd)
-          acc += double(blk[ab * ncd + cd]) * __ldg(Dm + (size_t)(c0 + cd / nd) * n + d0 + cd % nd);
-        atomicAdd(Jm + (size_t)(a0 + ab / nb) * n + b0 + ab % nb, 2.0 * s * acc);
-      }
-      for (int cd = lane; cd < ncd; cd += 32) {
-        double acc = 0.0;
-        for (int ab = 0; ab < na * nb; ++ab)
-          acc += double(blk[ab * ncd + cd]) * __ldg(Dm + (size_t)(a0 + ab / nb) * n + b0 + ab % nb);
-        atomicAdd(Jm + (size_t)(c0 + cd / nd) * n + d0 + cd % nd, 2.0 * s * acc);
-      }
-      // K[a][d] += v D[c][b]; K[a][c] += v D[d][b]
-      for (int idx = lane; idx < na * (nd + nc); idx += 32) {
-        const int a = idx / (nd + nc), r = idx % (nd + nc);
-        double acc = 0.0;
-        if (r < nd) {
-          for (int b = 0; b < nb; ++b)
-            for (int c = 0; c < nc; ++c)
-              acc += double(blk[(a * nb + b) * ncd + c * nd + r]) * __ldg(Dm + (size_t)(c0 + c) * n + b0 + b);
-          atomicAdd(Km + (size_t)(a0 + a) * n + d0 + r, s * acc);
-        } else {
-          const int c = r - nd;
-          for (int b = 0; b < nb; ++b)
-            for (int d = 0; d < nd; ++d)
-              acc += double(blk[(a * nb + b) * ncd + c * nd + d]) * __ldg(Dm + (size_t)(d0 + d) * n + b0 + b);
-          atomicAdd(Km + (size_t)(a0 + a) * n + c0 + c, s * acc);
-        }
-      }
-      // K[b][d] += v D[c][a]; K[b][c] += v D[d][a]
-      for (int idx = lane; idx < nb * (nd + nc); idx += 32) {
-        const int b = idx / (nd + nc), r = idx % (nd + nc);
-        double acc = 0.0;
-        if (r < nd) {
-          for (int a = 0; a < na; ++a)
-            for (int c = 0; c < nc; ++c)
-              acc += double(blk[(a * nb + b) * ncd + c * nd + r]) * __ldg(Dm + (size_t)(c0 + c) * n + a0 + a);
-          atomicAdd(Km + (size_t)(b0 + b) * n + d0 + r, s * acc);
-        } else {
-          const int c = r - nd;
-          for (int a = 0; a < na; ++a)
-            for (int d = 0; d < nd; ++d)
-              acc += double(blk[(a * nb + b) * ncd + c * nd + d]) * __ldg(Dm + (size_t)(d0 + d) * n + a0 + a);
-          atomicAdd(Km + (size_t)(b0 + b) * n + c0 + c, s * acc);
-        }
-      }
-    }
+    warp_digest_jk<T>(prm, sm->XB, na, nb, nc, nd, prm.ao[bp.a], prm.ao[bp.b], prm.ao[kp.a], prm.ao[kp.b], s, lane);
     __syncwarp();
   }
 }

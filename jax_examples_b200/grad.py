@@ -52,13 +52,19 @@ def _cart(engine: DirectERI, M: torch.Tensor) -> torch.Tensor:
     return engine._to_cart(M).contiguous()
 
 
-def grad_two_electron(engine: DirectERI, dens, j_scale: float, k_scale: float) -> torch.Tensor:
-    """1/2 sum Gamma d(ab|cd)/dR, (n_atom, 3)."""
+def grad_two_electron(engine: DirectERI, dens, j_scale: float, k_scale: float, dens_tau: float = 0.0,
+                      class_ms: Optional[list] = None) -> torch.Tensor:
+    """1/2 sum Gamma d(ab|cd)/dR, (n_atom, 3).  dens_tau > 0 skips quartets
+    whose Gamma bound times Q_ab Q_cd is below it; a list passed as class_ms
+    receives the 21 per-class kernel times (ms, classes serialised)."""
     D = torch.stack([_cart(engine, d) for d in dens]).contiguous()
     g = torch.zeros((len(engine.atom_Z), 3), dtype=torch.float64, device=engine.device)
+    ms = (ctypes.c_double * 21)() if class_ms is not None else None
     with torch.cuda.device(engine.device):
-        _abi.call("jqc_grad2e", engine._ctx, D.shape[0], _ptr(D), float(j_scale), float(k_scale), _ptr(g),
-                  _stream(engine.device))
+        _abi.call("jqc_grad2e_ex", engine._ctx, D.shape[0], _ptr(D), float(j_scale), float(k_scale),
+                  float(dens_tau), _ptr(g), _stream(engine.device), ms)
+    if class_ms is not None:
+        class_ms[:] = list(ms)
     return g
 
 
@@ -132,9 +138,12 @@ def _engine_for(mol, result, basis, engine):
     return DirectERI(basis, mol)
 
 
-def rhf_gradient(mol, result, basis=None, engine: Optional[DirectERI] = None, autograd: bool = False):
+def rhf_gradient(mol, result, basis=None, engine: Optional[DirectERI] = None, autograd: bool = False,
+                 dens_tau: float = 0.0):
     """Analytic RHF gradient (n_atoms, 3) in Hartree/bohr; same expression as
-    ``rhf_grad.py:106-211`` without finite differences."""
+    ``rhf_grad.py:106-211`` without finite differences.  dens_tau > 0 skips
+    two-electron quartets whose density-weighted bound is below it (the
+    mixed path's gradient; 0 = every Schwarz-surviving quartet)."""
     eng = _engine_for(mol, result, basis, engine)
     dev = eng.device
     st = result.state
@@ -148,7 +157,7 @@ def rhf_gradient(mol, result, basis=None, engine: Optional[DirectERI] = None, au
         (g,) = torch.autograd.grad(L, coords)
         return g
     g = nuclear_repulsion_gradient(mol.coords, mol.atomic_numbers).to(dev)
-    g = g + grad_one_electron(eng, D, W) + grad_two_electron(eng, [D], 1.0, 0.5)
+    g = g + grad_one_electron(eng, D, W) + grad_two_electron(eng, [D], 1.0, 0.5, dens_tau)
     return g
 
 

@@ -153,7 +153,7 @@ def test_launch_shapes_give_same_jk(threads, persistent, lane_prims):
     J0, K0 = torch.empty_like(D), torch.empty_like(D)
     eng.jk_into(D, J0, K0)
     cfg = eng.tuning()
-    assert cfg.shape == (21, 3) and np.all(cfg[:, 0] == 128)
+    assert cfg.shape == (21, 4) and np.all(cfg[:, 0] == 128)
     cfg[:, 0], cfg[:, 1], cfg[:, 2] = threads, lane_prims, persistent
     eng.set_tuning(cfg)
     np.testing.assert_array_equal(eng.tuning(), cfg)
@@ -168,6 +168,44 @@ def test_launch_shapes_give_same_jk(threads, persistent, lane_prims):
     bad[0, 0] = 96
     with pytest.raises(ValueError, match="threads"):
         eng.set_tuning(bad)
+    bad = cfg.copy()
+    bad[0, 3] = 1  # (ss|ss) has no column-engine kernel
+    with pytest.raises(ValueError, match="engine"):
+        eng.set_tuning(bad)
+    eng.close()
+
+
+@pytest.mark.parametrize("engine", [0, 1, 2])
+def test_engines_agree_on_high_l_classes(engine):
+    """Every engine that can evaluate a class gives the same J/K (FP64 1e-10,
+    FP32 split 1e-6)."""
+    batch = MoleculeBatch(_mols([3, 2], seed=7), BASIS)
+    eng = BatchedERI(batch)
+    rng = np.random.default_rng(8)
+    D = torch.tensor(_random_block_density(batch, rng), device=DEV)[None].contiguous()
+    J0, K0 = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J0, K0)
+    Jm0, Km0 = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, Jm0, Km0, "mixed", mixed_tau=1e-3)
+    cfg = eng.tuning()
+    from jax_examples_b200.engine import QUARTET_CLASSES
+
+    col = [12, 13, 14, 16, 17, 18, 19, 20]
+    for q in range(21):
+        L = sum(QUARTET_CLASSES[q])
+        ok = {0: L <= 6, 1: q in col, 2: True}[engine]
+        if ok:
+            cfg[q, 3] = engine
+    eng.set_tuning(cfg)
+    J, K = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J, K)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(J.cpu().numpy(), J0.cpu().numpy(), atol=1e-10, rtol=0)
+    np.testing.assert_allclose(K.cpu().numpy(), K0.cpu().numpy(), atol=1e-10, rtol=0)
+    eng.jk_into(D, J, K, "mixed", mixed_tau=1e-3)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(J.cpu().numpy(), Jm0.cpu().numpy(), atol=1e-6, rtol=0)
+    np.testing.assert_allclose(K.cpu().numpy(), Km0.cpu().numpy(), atol=1e-6, rtol=0)
     eng.close()
 
 
@@ -188,7 +226,7 @@ def test_autotune_keeps_results_and_uses_cache(tmp_path):
     np.testing.assert_allclose(J.cpu().numpy(), J0.cpu().numpy(), atol=1e-10, rtol=0)
     np.testing.assert_allclose(K.cpu().numpy(), K0.cpu().numpy(), atol=1e-10, rtol=0)
     lines = open(cache).read().strip().splitlines()
-    assert len(lines) == 1 and len(lines[0].split("\t")[1].split()) == 63
+    assert len(lines) == 1 and len(lines[0].split("\t")[1].split()) == 84
     eng.close()
     eng2 = BatchedERI(batch)
     assert eng2.autotune(D, J, K, "fp64", dens_tau=0.0, cache_path=cache) is True
@@ -224,3 +262,38 @@ def test_bfgs_batch_matches_single_molecule_runs():
         e_a = np.array([e for _, e in alone.trajectory])
         np.testing.assert_allclose(e_b, e_a, atol=1e-8, rtol=0)
         assert np.all(np.diff(e_b) <= 1e-10)  # Armijo steps never raise the energy
+
+
+def _set_grad_engines(eng, engine, classes):
+    for q in classes:
+        _abi.call("jqc_set_grad_engine", eng._ctx, q, engine)
+
+
+def test_gradient_engines_agree():
+    """The register, row and warp engines of the ERI-derivative adjoint give
+    the same two-electron gradient (1e-10 Eh/bohr) wherever they overlap."""
+    from jax_examples_b200.grad import grad_two_electron
+
+    mol = pb.water_cluster(3, seed=12, noise_angstrom=0.1)
+    bs = pb.build_basis_set(mol, BASIS)
+    eng = DirectERI(bs, mol, device=0, schwarz_tau=1e-12)
+    rng = np.random.default_rng(13)
+    n = bs.n_basis
+    a = rng.standard_normal((n, n)) * 0.05
+    D = torch.tensor(a + a.T, device=DEV)
+    engines = np.zeros(21, dtype=np.int32)
+    _abi.call("jqc_get_grad_engine", eng._ctx, engines.ctypes.data_as(_abi._ip))
+    g0 = grad_two_electron(eng, [D], 1.0, 0.5)
+    row = [11, 12, 13, 14, 15, 16, 18]
+    _set_grad_engines(eng, 2, range(21))  # warp engine everywhere
+    g_warp = grad_two_electron(eng, [D], 1.0, 0.5)
+    np.testing.assert_allclose(g_warp.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
+    _set_grad_engines(eng, 1, row)  # row engine where it exists
+    g_row = grad_two_electron(eng, [D], 1.0, 0.5)
+    np.testing.assert_allclose(g_row.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
+    _set_grad_engines(eng, 0, [11, 15])  # register kernels for the L <= 4 row classes
+    g_reg = grad_two_electron(eng, [D], 1.0, 0.5)
+    np.testing.assert_allclose(g_reg.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
+    with pytest.raises(ValueError, match="engine"):
+        _abi.call("jqc_set_grad_engine", eng._ctx, 20, 1)
+    eng.close()
