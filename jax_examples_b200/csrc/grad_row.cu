@@ -80,6 +80,147 @@ __device__ __forceinline__ void gr_hermite_R(double* R, const double* Rn, double
   }
 }
 
+struct F6 {
+  double v[6];
+};
+struct F3 {
+  double v[3];
+};
+
+// Bra-centre forces of row ab for the current primitive quartet:
+// Fg = Gamma_ab. contracted with the ket E, Z = Fg * R, then DA / DB.
+template <int LA, int LB, int LC, int LD>
+__device__ __noinline__ F6 row_bra(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
+  using S = GRowSmem<LA, LB, LC, LD>;
+  constexpr int LAB = S::LAB, LCD = S::LCD, NCD = S::NCD;
+  constexpr int NB = ncart(LB), ND = ncart(LD);
+  constexpr int NH1 = nherm(LAB + 1), NK0 = nherm(LCD);
+  const int ai = ab / NB, bi = ab - (ab / NB) * NB;
+  const int ax = cart_lx(LA, ai), ay = cart_ly(LA, ai), az = LA - ax - ay;
+  const int bx = cart_lx(LB, bi), by = cart_ly(LB, bi), bz = LB - bx - by;
+  const double* Gr = sm->G + ab * NCD;
+  double Fg[NK0];
+  static_for<NK0>([&](auto h_) { Fg[decltype(h_)::value] = 0.0; });
+  static_for<NCD>([&](auto cd_) {
+    constexpr int cd = decltype(cd_)::value, ci = cd / ND, di = cd % ND;
+    constexpr int cx = cart_lx(LC, ci), cy = cart_ly(LC, ci), cz = cart_lz(LC, ci);
+    constexpr int dx = cart_lx(LD, di), dy = cart_ly(LD, di), dz = cart_lz(LD, di);
+    const double w = Gr[cd];
+    static_for<cx + dx + 1>([&](auto t_) {
+      constexpr int t = decltype(t_)::value;
+      static_for<cy + dy + 1>([&](auto u_) {
+        constexpr int u = decltype(u_)::value;
+        const double wxy = w * sm->Fk[0][cx][dx][t] * sm->Fk[1][cy][dy][u];
+        static_for<cz + dz + 1>([&](auto v_) {
+          constexpr int v = decltype(v_)::value;
+          Fg[herm_index(t, u, v)] += wxy * sm->Fk[2][cz][dz][v];
+        });
+      });
+    });
+  });
+  double ex[LAB + 2], ey[LAB + 2], ez[LAB + 2];
+  double dax[LAB + 2], day[LAB + 2], daz[LAB + 2], dbx[LAB + 2], dby[LAB + 2], dbz[LAB + 2];
+  static_for<LAB + 2>([&](auto t_) {
+    constexpr int t = decltype(t_)::value;
+    ex[t] = sm->Eb[0][ax][bx][t];
+    ey[t] = sm->Eb[1][ay][by][t];
+    ez[t] = sm->Eb[2][az][bz][t];
+    dax[t] = sm->DA[0][ax][bx][t];
+    day[t] = sm->DA[1][ay][by][t];
+    daz[t] = sm->DA[2][az][bz][t];
+    dbx[t] = sm->DB[0][ax][bx][t];
+    dby[t] = sm->DB[1][ay][by][t];
+    dbz[t] = sm->DB[2][az][bz][t];
+  });
+  F6 out = {{0, 0, 0, 0, 0, 0}};
+  static_for<NH1>([&](auto h_) {
+    constexpr int h = decltype(h_)::value;
+    constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h);
+    double z = 0.0;
+    static_for<NK0>([&](auto k_) {
+      constexpr int k = decltype(k_)::value;
+      constexpr int ri = herm_index(t + gr_ht(k), u + gr_hu(k), v + gr_hv(k));
+      z += Fg[k] * sm->R[ri];
+    });
+    out.v[0] += dax[t] * ey[u] * ez[v] * z;
+    out.v[1] += ex[t] * day[u] * ez[v] * z;
+    out.v[2] += ex[t] * ey[u] * daz[v] * z;
+    out.v[3] += dbx[t] * ey[u] * ez[v] * z;
+    out.v[4] += ex[t] * dby[u] * ez[v] * z;
+    out.v[5] += ex[t] * ey[u] * dbz[v] * z;
+  });
+  return out;
+}
+
+// Ket-centre (C) force of row ab: W = E^ab * R, then Gamma with DC.
+template <int LA, int LB, int LC, int LD>
+__device__ __noinline__ F3 row_ket(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
+  using S = GRowSmem<LA, LB, LC, LD>;
+  constexpr int LAB = S::LAB, LCD = S::LCD, NCD = S::NCD;
+  constexpr int NB = ncart(LB), ND = ncart(LD);
+  constexpr int NH0 = nherm(LAB), NK1 = nherm(LCD + 1);
+  const int ai = ab / NB, bi = ab - (ab / NB) * NB;
+  const int ax = cart_lx(LA, ai), ay = cart_ly(LA, ai), az = LA - ax - ay;
+  const int bx = cart_lx(LB, bi), by = cart_ly(LB, bi), bz = LB - bx - by;
+  const double* Gr = sm->G + ab * NCD;
+  double Gab[NH0];
+  {
+    double ex[LAB + 1], ey[LAB + 1], ez[LAB + 1];
+    static_for<LAB + 1>([&](auto t_) {
+      constexpr int t = decltype(t_)::value;
+      ex[t] = sm->Eb[0][ax][bx][t];
+      ey[t] = sm->Eb[1][ay][by][t];
+      ez[t] = sm->Eb[2][az][bz][t];
+    });
+    static_for<NH0>([&](auto h_) {
+      constexpr int h = decltype(h_)::value;
+      Gab[h] = ex[gr_ht(h)] * ey[gr_hu(h)] * ez[gr_hv(h)];
+    });
+  }
+  double W[NK1];
+  static_for<NK1>([&](auto k_) {
+    constexpr int k = decltype(k_)::value;
+    constexpr int tk = gr_ht(k), uk = gr_hu(k), vk = gr_hv(k);
+    double w = 0.0;
+    static_for<NH0>([&](auto h_) {
+      constexpr int h = decltype(h_)::value;
+      w += Gab[h] * sm->R[herm_index(gr_ht(h) + tk, gr_hu(h) + uk, gr_hv(h) + vk)];
+    });
+    W[k] = w;
+  });
+  F3 out = {{0, 0, 0}};
+  static_for<NCD>([&](auto cd_) {
+    constexpr int cd = decltype(cd_)::value, ci = cd / ND, di = cd % ND;
+    constexpr int cx = cart_lx(LC, ci), cy = cart_ly(LC, ci), cz = cart_lz(LC, ci);
+    constexpr int dx = cart_lx(LD, di), dy = cart_ly(LD, di), dz = cart_lz(LD, di);
+    const double w = Gr[cd];
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    static_for<cx + dx + 2>([&](auto t_) {
+      constexpr int t = decltype(t_)::value;
+      static_for<cy + dy + 2>([&](auto u_) {
+        constexpr int u = decltype(u_)::value;
+        static_for<cz + dz + 2>([&](auto v_) {
+          constexpr int v = decltype(v_)::value;
+          constexpr int over = (t > cx + dx) + (u > cy + dy) + (v > cz + dz);
+          if constexpr (over <= 1) {
+            const double wk = W[herm_index(t, u, v)];
+            if constexpr (u <= cy + dy && v <= cz + dz)
+              sx += sm->DC[0][cx][dx][t] * sm->Fk[1][cy][dy][u] * sm->Fk[2][cz][dz][v] * wk;
+            if constexpr (t <= cx + dx && v <= cz + dz)
+              sy += sm->Fk[0][cx][dx][t] * sm->DC[1][cy][dy][u] * sm->Fk[2][cz][dz][v] * wk;
+            if constexpr (t <= cx + dx && u <= cy + dy)
+              sz += sm->Fk[0][cx][dx][t] * sm->Fk[1][cy][dy][u] * sm->DC[2][cz][dz][v] * wk;
+          }
+        });
+      });
+    });
+    out.v[0] += w * sx;
+    out.v[1] += w * sy;
+    out.v[2] += w * sz;
+  });
+  return out;
+}
+
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(32 * kGRowWarps) grad_row_kernel(const GradParams prm) {
   using S = GRowSmem<LA, LB, LC, LD>;
@@ -185,110 +326,14 @@ __global__ void __launch_bounds__(32 * kGRowWarps) grad_row_kernel(const GradPar
         }
         __syncwarp();
         gr_hermite_R<L + 1>(sm->R, sm->Rn, X, Y, Z, lane);
+#pragma unroll 1
         for (int ab = lane; ab < NAB; ab += 32) {
-          const int ai = ab / NB, bi = ab - (ab / NB) * NB;
-          const int ax = cart_lx(LA, ai), ay = cart_ly(LA, ai), az = LA - ax - ay;
-          const int bx = cart_lx(LB, bi), by = cart_ly(LB, bi), bz = LB - bx - by;
-          const double* Gr = sm->G + ab * NCD;
-          // Fg[h'] = sum_cd Gamma_abcd F^cd_h'
-          double Fg[NK0];
-          static_for<NK0>([&](auto h_) { Fg[decltype(h_)::value] = 0.0; });
-          static_for<NCD>([&](auto cd_) {
-            constexpr int cd = decltype(cd_)::value, ci = cd / ND, di = cd % ND;
-            constexpr int cx = cart_lx(LC, ci), cy = cart_ly(LC, ci), cz = cart_lz(LC, ci);
-            constexpr int dx = cart_lx(LD, di), dy = cart_ly(LD, di), dz = cart_lz(LD, di);
-            const double w = Gr[cd];
-            static_for<cx + dx + 1>([&](auto t_) {
-              constexpr int t = decltype(t_)::value;
-              static_for<cy + dy + 1>([&](auto u_) {
-                constexpr int u = decltype(u_)::value;
-                const double wxy = w * sm->Fk[0][cx][dx][t] * sm->Fk[1][cy][dy][u];
-                static_for<cz + dz + 1>([&](auto v_) {
-                  constexpr int v = decltype(v_)::value;
-                  Fg[herm_index(t, u, v)] += wxy * sm->Fk[2][cz][dz][v];
-                });
-              });
-            });
-          });
-          // bra rows of this lane
-          double ex[LAB + 2], ey[LAB + 2], ez[LAB + 2];
-          static_for<LAB + 2>([&](auto t_) {
-            constexpr int t = decltype(t_)::value;
-            ex[t] = sm->Eb[0][ax][bx][t];
-            ey[t] = sm->Eb[1][ay][by][t];
-            ez[t] = sm->Eb[2][az][bz][t];
-          });
-          {
-            // Z[h] = sum_h' Fg[h'] R_{h+h'}, contracted at once with DA, DB
-            double dax[LAB + 2], day[LAB + 2], daz[LAB + 2], dbx[LAB + 2], dby[LAB + 2], dbz[LAB + 2];
-            static_for<LAB + 2>([&](auto t_) {
-              constexpr int t = decltype(t_)::value;
-              dax[t] = sm->DA[0][ax][bx][t];
-              day[t] = sm->DA[1][ay][by][t];
-              daz[t] = sm->DA[2][az][bz][t];
-              dbx[t] = sm->DB[0][ax][bx][t];
-              dby[t] = sm->DB[1][ay][by][t];
-              dbz[t] = sm->DB[2][az][bz][t];
-            });
-            static_for<NH1>([&](auto h_) {
-              constexpr int h = decltype(h_)::value;
-              constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h);
-              double z = 0.0;
-              static_for<NK0>([&](auto k_) {
-                constexpr int k = decltype(k_)::value;
-                constexpr int ri = herm_index(t + gr_ht(k), u + gr_hu(k), v + gr_hv(k));
-                z += Fg[k] * sm->R[ri];
-              });
-              g[0] += dax[t] * ey[u] * ez[v] * z;
-              g[1] += ex[t] * day[u] * ez[v] * z;
-              g[2] += ex[t] * ey[u] * daz[v] * z;
-              g[3] += dbx[t] * ey[u] * ez[v] * z;
-              g[4] += ex[t] * dby[u] * ez[v] * z;
-              g[5] += ex[t] * ey[u] * dbz[v] * z;
-            });
-          }
-          // W[h'] = sum_h E^ab_h R_{h+h'}, then the ket derivative
-          double W[NK1];
-          static_for<NK1>([&](auto k_) {
-            constexpr int k = decltype(k_)::value;
-            constexpr int tk = gr_ht(k), uk = gr_hu(k), vk = gr_hv(k);
-            double w = 0.0;
-            static_for<NH0>([&](auto h_) {
-              constexpr int h = decltype(h_)::value;
-              constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h);
-              w += ex[t] * ey[u] * ez[v] * sm->R[herm_index(t + tk, u + uk, v + vk)];
-            });
-            W[k] = w;
-          });
-          static_for<NCD>([&](auto cd_) {
-            constexpr int cd = decltype(cd_)::value, ci = cd / ND, di = cd % ND;
-            constexpr int cx = cart_lx(LC, ci), cy = cart_ly(LC, ci), cz = cart_lz(LC, ci);
-            constexpr int dx = cart_lx(LD, di), dy = cart_ly(LD, di), dz = cart_lz(LD, di);
-            const double w = Gr[cd];
-            double sx = 0.0, sy = 0.0, sz = 0.0;
-            static_for<cx + dx + 2>([&](auto t_) {
-              constexpr int t = decltype(t_)::value;
-              static_for<cy + dy + 2>([&](auto u_) {
-                constexpr int u = decltype(u_)::value;
-                static_for<cz + dz + 2>([&](auto v_) {
-                  constexpr int v = decltype(v_)::value;
-                  constexpr int over = (t > cx + dx) + (u > cy + dy) + (v > cz + dz);
-                  if constexpr (over <= 1) {
-                    const double wk = W[herm_index(t, u, v)];
-                    if constexpr (u <= cy + dy && v <= cz + dz)
-                      sx += sm->DC[0][cx][dx][t] * sm->Fk[1][cy][dy][u] * sm->Fk[2][cz][dz][v] * wk;
-                    if constexpr (t <= cx + dx && v <= cz + dz)
-                      sy += sm->Fk[0][cx][dx][t] * sm->DC[1][cy][dy][u] * sm->Fk[2][cz][dz][v] * wk;
-                    if constexpr (t <= cx + dx && u <= cy + dy)
-                      sz += sm->Fk[0][cx][dx][t] * sm->Fk[1][cy][dy][u] * sm->DC[2][cz][dz][v] * wk;
-                  }
-                });
-              });
-            });
-            g[6] += w * sx;
-            g[7] += w * sy;
-            g[8] += w * sz;
-          });
+          const F6 fb = row_bra<LA, LB, LC, LD>(sm, ab);
+          const F3 fc = row_ket<LA, LB, LC, LD>(sm, ab);
+#pragma unroll
+          for (int k = 0; k < 6; ++k) g[k] += fb.v[k];
+#pragma unroll
+          for (int k = 0; k < 3; ++k) g[6 + k] += fc.v[k];
         }
         __syncwarp();
       }
@@ -332,9 +377,7 @@ static cudaError_t launch_grad_row_class(const GradParams& p, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// Gradient classes with a row-engine kernel (bra pair dp or dd; the dd bras
-// with a pp/dp/dd ket stay on the warp engine: their fully unrolled row body
-// exceeds what the register allocator handles).
+// Gradient classes with a row-engine kernel (bra pair dp or dd).
 #define JQC_FOR_GRAD_ROW_CLASSES(X) \
   X(11, 2, 1, 1, 0)                 \
   X(12, 2, 1, 1, 1)                 \
@@ -342,7 +385,10 @@ static cudaError_t launch_grad_row_class(const GradParams& p, cudaStream_t s) {
   X(14, 2, 1, 2, 1)                 \
   X(15, 2, 2, 0, 0)                 \
   X(16, 2, 2, 1, 0)                 \
-  X(18, 2, 2, 2, 0)
+  X(17, 2, 2, 1, 1)                 \
+  X(18, 2, 2, 2, 0)                 \
+  X(19, 2, 2, 2, 1)                 \
+  X(20, 2, 2, 2, 2)
 
 bool has_grad_row_class(int qc) {
   switch (qc) {

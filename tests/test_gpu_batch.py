@@ -284,7 +284,7 @@ def test_gradient_engines_agree():
     engines = np.zeros(21, dtype=np.int32)
     _abi.call("jqc_get_grad_engine", eng._ctx, engines.ctypes.data_as(_abi._ip))
     g0 = grad_two_electron(eng, [D], 1.0, 0.5)
-    row = [11, 12, 13, 14, 15, 16, 18]
+    row = [11, 12, 13, 14, 15, 16, 17, 18, 19, 20]
     _set_grad_engines(eng, 2, range(21))  # warp engine everywhere
     g_warp = grad_two_electron(eng, [D], 1.0, 0.5)
     np.testing.assert_allclose(g_warp.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
@@ -295,5 +295,5 @@ def test_gradient_engines_agree():
     g_reg = grad_two_electron(eng, [D], 1.0, 0.5)
     np.testing.assert_allclose(g_reg.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
     with pytest.raises(ValueError, match="engine"):
-        _abi.call("jqc_set_grad_engine", eng._ctx, 20, 1)
+        _abi.call("jqc_set_grad_engine", eng._ctx, 0, 1)  # (ss|ss) has no row kernel
     eng.close()
