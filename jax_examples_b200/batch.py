@@ -47,6 +47,10 @@ from .scf import DIIS, diis_error, symmetric_orthogonalization
 # 1e-30 Eh: the builds stay FP64-exact for every active molecule.
 BATCH_DENS_TAU = 1e-30
 
+# Density screening of the gradient on the mixed path: the skipped quartets
+# change a (H2O)16 gradient by ~1e-6 Eh/bohr, inside the 1e-5 tolerance.
+MIXED_GRAD_TAU = 1e-10
+
 
 class _Nuclei:
     """Nuclei of a batch in the form DirectERI reads (coords, charges)."""
@@ -258,6 +262,139 @@ class BatchSCF(NamedTuple):
     record: dict
 
 
+class _BatchFock:
+    """J/K builds of a batch under the SCF precision policy of
+    :class:`jax_examples_b200.fock.FockBuilder`, on fixed buffers replayed as
+    CUDA graphs (one graph per build kind).
+
+    * ``precision="fp64"``: a full FP64 build every iteration (screening only
+      drops the quartets of converged molecules, whose density blocks are
+      zero).
+    * ``precision="mixed"`` with ``incremental``: the first build is a full
+      mixed build (FP32 for Q_ij Q_kl < mixed_tau); then each build contracts
+      the density change of the active molecules (J, K are linear in D) with
+      density screening at ``mixed_dens_tau``, a full rebuild every
+      ``rebuild_every`` builds.  Once the largest DIIS error of the active
+      molecules is below ``fp64_switch`` it switches to a full FP64 build and
+      incremental FP64 builds at the tight threshold 1e-12; convergence is
+      accepted only after ``fp64_tail_iters`` FP64 builds.
+    """
+
+    def __init__(self, eng: BatchedERI, batch: MoleculeBatch, config: CalcConfig, use_graph: bool,
+                 rebuild_every: int = 8):
+        self.eng, self.batch, self.config = eng, batch, config
+        self.cart = eng.cartesian
+        self.use_graph = use_graph and self.cart
+        self.mixed = config.precision == "mixed"
+        self.incremental = bool(config.incremental) and self.mixed
+        self.mixed_tau = float(config.mixed_tau)
+        self.phase = "mixed" if self.mixed else "fp64"
+        self.rebuild_every = rebuild_every
+        self.fp64_builds = 0
+        self.since_full = 0
+        self.prev = None  # densities of the last build, per molecule
+        self.events = []
+        self.graphs = {}
+        self.log = {"builds_mixed": 0, "builds_fp64": 0, "incremental_builds": 0}
+        self.D, self.J, self.K = eng.buffers(1)
+        self.Jacc = torch.zeros_like(self.J[0])
+        self.Kacc = torch.zeros_like(self.K[0])
+
+    def _settings(self, incremental: bool):
+        if self.phase == "mixed":
+            return "mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU) if incremental else BATCH_DENS_TAU
+        return "fp64", 1e-12 if incremental else BATCH_DENS_TAU
+
+    def _launch(self, incremental: bool):
+        prec, tau = self._settings(incremental)
+        key = (prec, tau)
+        if self.use_graph:
+            if key not in self.graphs:
+                self.graphs[key] = self.eng.capture_jk(self.D, self.J, self.K, prec, self.mixed_tau, tau)
+            self.eng.launch(self.graphs[key])
+        else:
+            self.eng.jk_into(self.D, self.J, self.K, prec, self.mixed_tau, tau)
+        self.log["builds_mixed" if prec == "mixed" else "builds_fp64"] += 1
+        if prec == "fp64" and self.switched:
+            self.fp64_builds += 1
+
+    @property
+    def switched(self) -> bool:
+        return self.mixed and self.phase == "fp64"
+
+    def prepare(self, dens: dict, autotune: bool, tune_cache: Optional[str]) -> None:
+        """Work lists, autotuning and graph capture before the timed builds."""
+        if not self.cart:
+            return
+        for m, d in dens.items():
+            self.batch.block(self.D[0], m).copy_(d)
+        prec, tau = self._settings(False)
+        if autotune:
+            self.eng.autotune(self.D, self.J, self.K, prec, self.mixed_tau, tau, cache_path=tune_cache)
+        if self.use_graph:
+            kinds = [(prec, tau)]
+            if self.mixed:
+                kinds += [("fp64", BATCH_DENS_TAU)]
+            if self.incremental:
+                kinds += [("mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU)), ("fp64", 1e-12)]
+            for p_, t_ in kinds:
+                self.graphs[(p_, t_)] = self.eng.capture_jk(self.D, self.J, self.K, p_, self.mixed_tau, t_)
+
+    def build(self, dens: dict) -> dict:
+        """(J_m, K_m) of the molecules in dens."""
+        b = self.batch
+        if not self.cart:
+            Dfull = torch.zeros((self.eng.n_basis, self.eng.n_basis), dtype=torch.float64, device=self.eng.device)
+            for m, d in dens.items():
+                b.block(Dfull, m).copy_(d)
+            prec, tau = self._settings(False)
+            J, K = self.eng.engine.jk(Dfull, precision=prec, mixed_tau=self.mixed_tau, dens_tau=tau)
+            self.log["builds_mixed" if prec == "mixed" else "builds_fp64"] += 1
+            if prec == "fp64" and self.switched:
+                self.fp64_builds += 1
+            return {m: (b.block(J, m), b.block(K, m)) for m in dens}
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        inc = (self.incremental and self.prev is not None and self.since_full < self.rebuild_every
+               and set(dens) <= set(self.prev))
+        self.D.zero_()
+        if inc:
+            for m, d in dens.items():
+                b.block(self.D[0], m).copy_(d - self.prev[m])
+            self._launch(True)
+            self.Jacc += self.J[0]
+            self.Kacc += self.K[0]
+            self.since_full += 1
+            self.log["incremental_builds"] += 1
+        else:
+            for m, d in dens.items():
+                b.block(self.D[0], m).copy_(d)
+            self._launch(False)
+            self.Jacc.copy_(self.J[0])
+            self.Kacc.copy_(self.K[0])
+            self.since_full = 0
+        if self.incremental:
+            self.prev = dict(dens)
+        e1.record()
+        self.events.append((e0, e1))
+        return {m: (b.block(self.Jacc, m), b.block(self.Kacc, m)) for m in dens}
+
+    def observe(self, err_max: float) -> None:
+        if self.phase == "mixed" and err_max < float(self.config.fp64_switch):
+            self.phase = "fp64"
+            self.prev = None  # next build: a full FP64 build
+
+    def converged_ok(self) -> bool:
+        return not self.mixed or (self.phase == "fp64" and self.fp64_builds >= int(self.config.fp64_tail_iters))
+
+    def seconds(self) -> float:
+        if not self.events:
+            return 0.0
+        self.events[-1][1].synchronize()
+        return sum(a.elapsed_time(c) for a, c in self.events) * 1e-3
+
+
 def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, engine: Optional[BatchedERI] = None,
                   use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None) -> BatchSCF:
     """Closed-shell SCF of every molecule of the batch, in lock step.
@@ -266,16 +403,15 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     :func:`jax_examples_b200.scf.run_rhf`): core-Hamiltonian guess, Loewdin
     X = S^-1/2, F0 from the guess density, DIIS, converged when
     dE < scf_conv and max|DIIS error| < max(scf_conv, 1e-6).  All molecules
-    share each Fock build (one graph replay of the batch J/K); a converged
-    molecule keeps its state and its density block is zeroed for the
-    remaining builds.
+    share each Fock build (one graph replay of the batch J/K, see
+    :class:`_BatchFock` for the precision policy of ``config.precision``); a
+    converged molecule keeps its state and leaves the builds.
     """
     config = config or CalcConfig()
     for mol in batch.mols:
         if mol.spin != 0 or mol.n_electrons % 2 != 0:
             raise ValueError("run_rhf_batch requires closed-shell molecules (spin 0, even electron count)")
     eng = engine or BatchedERI(batch, schwarz_tau=config.schwarz_tau)
-    dev = eng.device
     M = len(batch)
     t_setup = time.perf_counter()
     S_all, T_all, V_all = eng.engine.one_electron()
@@ -285,46 +421,18 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     X = [symmetric_orthogonalization(s) for s in S]
     n_occ = [mol.n_electrons // 2 for mol in batch.mols]
     E_nuc = [nuclear_repulsion_energy(mol) for mol in batch.mols]
-
-    Dbuf, Jbuf, Kbuf = eng.buffers(1)
-    cart = eng.cartesian
-    graph = None
-    events = []
+    fb = _BatchFock(eng, batch, config, use_graph)
 
     def fock(dens: dict) -> dict:
-        """F_m = H_m + J_m - K_m / 2 for the molecules in dens (others zeroed)."""
-        if cart:
-            Dbuf.zero_()
-            for m, d in dens.items():
-                batch.block(Dbuf[0], m).copy_(d)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            if graph is not None:
-                eng.launch(graph)
-            else:
-                eng.jk_into(Dbuf, Jbuf, Kbuf, "fp64", dens_tau=BATCH_DENS_TAU)
-            e1.record()
-            events.append((e0, e1))
-            J, K = Jbuf[0], Kbuf[0]
-        else:
-            Dfull = torch.zeros((eng.n_basis, eng.n_basis), dtype=torch.float64, device=dev)
-            for m, d in dens.items():
-                batch.block(Dfull, m).copy_(d)
-            J, K = eng.engine.jk(Dfull, dens_tau=BATCH_DENS_TAU)
-        return {m: H[m] + batch.block(J, m) - 0.5 * batch.block(K, m) for m in dens}
+        jk = fb.build(dens)
+        return {m: H[m] + jk[m][0] - 0.5 * jk[m][1] for m in dens}
 
     # core guess (rhf.py:111-121)
     all_m = list(range(M))
     dg = _diag_groups(H, X, all_m)
     D = {m: 2.0 * dg[m][1][:, :n_occ[m]] @ dg[m][1][:, :n_occ[m]].T for m in all_m}
-    if cart and (use_graph or autotune):
-        for m in all_m:
-            batch.block(Dbuf[0], m).copy_(D[m])
-        if autotune:
-            eng.autotune(Dbuf, Jbuf, Kbuf, "fp64", dens_tau=BATCH_DENS_TAU, cache_path=tune_cache)
-        if use_graph:
-            graph = eng.capture_jk(Dbuf, Jbuf, Kbuf, "fp64", dens_tau=BATCH_DENS_TAU)
+    fb.prepare(D, autotune, tune_cache)
+    torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
     F = fock(D)
     dg = _diag_groups(F, X, all_m)
@@ -336,12 +444,10 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     iters = [0] * M
     converged = [False] * M
     active = list(all_m)
-    n_builds = 1
     for _ in range(config.max_scf_iter):
         if not active:
             break
         Fn = fock({m: D[m] for m in active})
-        n_builds += 1
         if config.damping > 0.0:
             Fn = {m: (1.0 - config.damping) * Fn[m] + config.damping * F[m] for m in active}
         err = {m: diis_error(Fn[m], D[m], S[m], X[m]) for m in active}
@@ -354,37 +460,39 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
             iters[m] += 1
         En = torch.stack([0.5 * torch.sum(D[m] * (H[m] + Fx[m])) for m in active]).cpu().numpy()
         emax = torch.stack([torch.max(torch.abs(err[m])) for m in active]).cpu().numpy()
+        fb.observe(float(emax.max()))
+        ok = fb.converged_ok()
         still = []
         for i, m in enumerate(active):
             E[m] = En[i]
             dE = abs(E[m] - last[m])
             last[m] = E[m]
-            if dE < config.scf_conv and emax[i] < max(config.scf_conv, 1e-6):
+            if ok and dE < config.scf_conv and emax[i] < max(config.scf_conv, 1e-6):
                 converged[m] = True
             else:
                 still.append(m)
         active = still
-    jk_s = 0.0
-    if events:
-        events[-1][1].synchronize()
-        jk_s = sum(a.elapsed_time(b) for a, b in events) * 1e-3
-    record = {"fock_builds": n_builds, "jk_seconds": jk_s, "setup_seconds": setup_s, "graph": graph is not None,
-              "autotuned": bool(autotune), "n_molecules": M, "n_basis": batch.n_basis}
+    record = dict(fb.log, fock_builds=sum(fb.log[k] for k in ("builds_mixed", "builds_fp64")),
+                  jk_seconds=fb.seconds(), setup_seconds=setup_s, graph=bool(fb.graphs), autotuned=bool(autotune),
+                  n_molecules=M, n_basis=batch.n_basis, precision=config.precision,
+                  incremental=fb.incremental)
     results = []
     for m in all_m:
         st = SCFState(density=D[m], fock=F[m], coefficients=C[m], orbital_energies=eps[m], energy=float(E[m]),
                       iteration=iters[m])
         results.append(SCFResult(converged=converged[m], state=st, energy=float(E[m]) + E_nuc[m],
                                  E_elec=float(E[m]), E_nuc=E_nuc[m], n_iterations=iters[m], S=S[m], H_core=H[m],
-                                 ERI=None, precision={"precision": "fp64", "batched": True}))
+                                 ERI=None, precision={"precision": config.precision, "batched": True}))
     return BatchSCF(results=results, engine=eng, record=record)
 
 
-def rhf_gradient_batch(batch: MoleculeBatch, scf: BatchSCF, timing: Optional[dict] = None) -> List[torch.Tensor]:
+def rhf_gradient_batch(batch: MoleculeBatch, scf: BatchSCF, timing: Optional[dict] = None,
+                       dens_tau: float = 0.0) -> List[torch.Tensor]:
     """Analytic RHF gradients (n_atoms_m, 3) of every molecule of the batch:
     one ``jqc_grad2e`` and one ``jqc_grad1e`` call over the block-diagonal
     densities (the per-molecule expression of
-    :func:`jax_examples_b200.grad.rhf_gradient`)."""
+    :func:`jax_examples_b200.grad.rhf_gradient`; dens_tau > 0 screens the
+    two-electron quartets by their density-weighted bound)."""
     eng = scf.engine
     dev = eng.device
     n = eng.n_basis
@@ -398,7 +506,7 @@ def rhf_gradient_batch(batch: MoleculeBatch, scf: BatchSCF, timing: Optional[dic
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    g = grad_one_electron(eng.engine, D, W) + grad_two_electron(eng.engine, [D], 1.0, 0.5)
+    g = grad_one_electron(eng.engine, D, W) + grad_two_electron(eng.engine, [D], 1.0, 0.5, dens_tau)
     e1.record()
     e1.synchronize()
     if timing is not None:
@@ -486,8 +594,9 @@ def energies_and_gradients(mols: Sequence, basis: str = "syn-6-31g*", config: Op
     """RHF energies and analytic gradients of many molecules in one batch:
     ``[(energy, gradient (n_atoms, 3) ndarray, SCFResult)]``."""
     batch = MoleculeBatch(mols, basis)
+    config = config or CalcConfig()
     scf = run_rhf_batch(batch, config, use_graph=use_graph, autotune=autotune, tune_cache=tune_cache)
-    grads = rhf_gradient_batch(batch, scf, timing)
+    grads = rhf_gradient_batch(batch, scf, timing, MIXED_GRAD_TAU if config.precision == "mixed" else 0.0)
     if timing is not None:
         timing["jk_seconds"] = timing.get("jk_seconds", 0.0) + scf.record["jk_seconds"]
         timing["fock_builds"] = timing.get("fock_builds", 0) + scf.record["fock_builds"]

@@ -135,6 +135,8 @@ class CalcConfig(_Replace):
                     convergence the remaining iterations use incremental FP64
                     builds; at least this many FP64 iterations are run.
     incremental:    build F from the density change dD when true.
+    mixed_dens_tau: density-screening threshold of the incremental builds
+                    in the mixed phase (the FP64 tail uses 1e-12).
     """
 
     method: str = "rhf"
@@ -153,6 +155,7 @@ class CalcConfig(_Replace):
     fp64_tail_iters: int = 2
     fp64_switch: float = 1e-5
     incremental: bool = True
+    mixed_dens_tau: float = 1e-9
 
 
 def make_molecule(elements, coords, atomic_numbers, charge: int = 0, spin: int = 0) -> Molecule:

@@ -367,22 +367,28 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
       }
     }
   }
-  // Longest tasks first inside each class launch (cost = lane primitive quartets).
-  for (int prec = 0; prec < 2; ++prec)
-    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-      auto& v = lists[prec][qc];
-      std::stable_sort(v.begin(), v.end(), [&](const Task& x, const Task& y) {
-        const long long cx = (long long)((x.flags >> 16) - (x.flags & 0xffff)) * c->pairs[x.ket0].npp;
-        const long long cy = (long long)((y.flags >> 16) - (y.flags & 0xffff)) * c->pairs[y.ket0].npp;
-        return cx > cy;
-      });
-    }
+  // Longest tasks first inside each class launch (cost = lane primitive
+  // quartets = bra primitive chunk x ket primitive pairs): a stable counting
+  // sort on the cost, linear in the number of tasks.
   ts.h.clear();
+  std::vector<int> cost, count;
   for (int prec = 0; prec < 2; ++prec)
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      const auto& v = lists[prec][qc];
       ts.off[prec][qc] = (int)ts.h.size();
-      ts.cnt[prec][qc] = (int)lists[prec][qc].size();
-      ts.h.insert(ts.h.end(), lists[prec][qc].begin(), lists[prec][qc].end());
+      ts.cnt[prec][qc] = (int)v.size();
+      cost.resize(v.size());
+      int cmax = 0;
+      for (size_t k = 0; k < v.size(); ++k) {
+        cost[k] = ((v[k].flags >> 16) - (v[k].flags & 0xffff)) * c->pairs[v[k].ket0].npp;
+        cmax = std::max(cmax, cost[k]);
+      }
+      count.assign(cmax + 2, 0);
+      for (size_t k = 0; k < v.size(); ++k) ++count[cmax - cost[k] + 1];  // descending cost
+      for (int b = 1; b <= cmax + 1; ++b) count[b] += count[b - 1];
+      const size_t base = ts.h.size();
+      ts.h.resize(base + v.size());
+      for (size_t k = 0; k < v.size(); ++k) ts.h[base + count[cmax - cost[k]]++] = v[k];
     }
   JQC_CUDA_CHECK(ts.d.upload(ts.h, s));
   ts.n_quartets[0] = nq[0];
@@ -1339,8 +1345,10 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
     drop_jk_tasks(c);
     return ensure_jk_tasks(c, precision_mode, mixed_tau, s);
   };
-  // 2. engine of every class (register / column / warp where available)
-  for (int e = kEngineReg; e <= kEngineWarp; ++e) {
+  // 2. engine of every class, register or column kernels where a class has
+  // both (the runtime-class warp engine is never the faster one; it stays
+  // the fallback of classes without either)
+  for (int e = kEngineReg; e <= kEngineCol; ++e) {
     for (int qc = 0; qc < kNumQuartetClasses; ++qc)
       c->tune[qc] = ClassTune{128, kMaxLanePrims, 0, engine_valid(e, qc) ? e : default_engine(qc)};
     rc = rebuild();

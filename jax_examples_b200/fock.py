@@ -12,9 +12,14 @@ the precision policy of the mixed path:
   (FP64 accumulation), and with ``incremental=True`` each build contracts only
   the density change dD = D - D_prev (J, K are linear in D) with density-
   weighted screening, the error of which is reset by a full rebuild every
-  ``rebuild_every`` builds.  When the SCF error drops below ``fp64_switch`` the
-  builder switches to full FP64 builds, and convergence is only accepted after
-  ``fp64_tail_iters`` of them: the final energy is an FP64 energy.
+  ``rebuild_every`` builds.  In this phase the incremental builds screen at
+  ``mixed_dens_tau`` (1e-9: the early Fock matrices only steer the next
+  density; a threshold that follows the DIIS error upward of that slowed the
+  convergence more than it saved).  When the SCF error
+  drops below ``fp64_switch`` the builder switches to FP64 with a full
+  rebuild and then tight-threshold incremental FP64 builds, and convergence
+  is only accepted after ``fp64_tail_iters`` of them: the final energy is an
+  FP64 energy.
 """
 
 from __future__ import annotations
@@ -95,6 +100,7 @@ class FockBuilder:
         self.fp64_switch = float(getattr(config, "fp64_switch", 1e-5))
         self.rebuild_every = rebuild_every
         self.dens_tau = dens_tau
+        self.mixed_dens_tau = float(getattr(config, "mixed_dens_tau", 1e-9))
         self.phase = "mixed" if (self.precision == "mixed" and self.direct) else "fp64"
         self.fp64_builds_after_switch = 0
         self.switched = self.phase == "fp64"
@@ -122,7 +128,8 @@ class FockBuilder:
         use_inc = self.incremental and self._prev is not None and self._since_full < self.rebuild_every
         if use_inc and self._prev[0].shape == D.shape:
             dD = D - self._prev[0]
-            dJ, dK = self.eri.jk(dD, precision=prec, mixed_tau=self.mixed_tau, dens_tau=self.dens_tau)
+            tau = max(self.mixed_dens_tau, self.dens_tau) if prec == "mixed" else self.dens_tau
+            dJ, dK = self.eri.jk(dD, precision=prec, mixed_tau=self.mixed_tau, dens_tau=tau)
             J = self._prev[1] + dJ
             K = self._prev[2] + dK
             self._since_full += 1
