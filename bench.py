@@ -51,10 +51,9 @@ WORKLOAD = (f"(H2O){N_WATERS} lattice 2.9A, 6-31G*-shaped Cartesian ({19 * N_WAT
 
 
 def _dist():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from jax_examples_b200.dist import env_ranks
+
+    return env_ranks()
 
 
 # ------------------------------------------------------------------- CPU leg
@@ -268,6 +267,7 @@ def run_ours(args):
 
     from jax_examples_b200 import CalcConfig, DirectERI, _abi, compute_integrals, run_scf
     from jax_examples_b200 import basis as pb
+    from jax_examples_b200 import dist as jdist
     from jax_examples_b200 import flops
     from jax_examples_b200.engine import QUARTET_CLASSES, fp_peak
 
@@ -321,10 +321,7 @@ def run_ours(args):
             times.append(e0.elapsed_time(e1))
     barrier()
     ms = float(np.sum(times)) / args.steps
-    t_max = torch.tensor([ms], device=dev)
-    if dist is not None:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max = float(t_max.item())
+    ms_max = jdist.max_over_ranks(ms)
     value = nq * world / (ms_max * 1e-3)
 
     # --- end to end through the C ABI with host buffers
@@ -358,10 +355,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         e2e_times.append(e0.elapsed_time(e1))
     e2e_ms = float(np.mean(e2e_times))
-    t_e = torch.tensor([e2e_ms], device=dev)
-    if dist is not None:
-        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
-    e2e_value = nq * world / (float(t_e.item()) * 1e-3)
+    e2e_value = nq * world / (jdist.max_over_ranks(e2e_ms) * 1e-3)
 
     if rank != 0:
         if dist is not None:

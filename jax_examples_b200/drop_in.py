@@ -10,7 +10,13 @@ reference's two-electron entry points to this package's device path:
   tensor from the device kernels, as a host array;
 * ``jax_qc.scf.fock.build_fock_rhf`` / ``build_fock_uhf`` (``fock.py:41-79``)
   and their by-name imports in ``scf/rhf.py:37`` and ``scf/uhf.py:51``;
-* ``jax_qc.scf.guess.core_guess_uhf`` (its inlined J/K, ``guess.py:87-88``).
+* ``jax_qc.scf.guess.core_guess_uhf`` (its inlined J/K, ``guess.py:87-88``);
+* ``jax_qc.grad.rhf_grad.rhf_gradient`` (``rhf_grad.py:106-211``) and its
+  by-name imports in ``grad/interface.py:17``, ``geomopt/optimizer.py:30``
+  and ``geomopt/hessian.py:21``: the analytic gradient (ERI-derivative
+  adjoint kernel, one-electron derivative kernels) in place of the finite
+  differences of whole integral sets, so the reference's BFGS
+  (``optimizer.py:79-209``) and FD Hessian run on it unchanged.
 
 Matrices are handed back in the caller's array type (NumPy, or JAX arrays
 when ``jax`` is importable: a DLPack hand-off of the device tensor), so the
@@ -116,6 +122,23 @@ def _patched_einsum(orig):
     return einsum
 
 
+def rhf_gradient(mol, result, basis_name: str = "sto-3g", step_size: float = 1e-4):
+    """Drop-in for ``jax_qc.grad.rhf_grad.rhf_gradient`` (same signature;
+    ``step_size`` is unused: the gradient is analytic)."""
+    from .grad import rhf_gradient as ours
+
+    eng = getattr(result, "ERI", None)
+    if not isinstance(eng, DirectERI):
+        build = sys.modules.get("jax_qc.basis.build")
+        if build is None:
+            import importlib
+
+            build = importlib.import_module("jax_qc.basis.build")
+        eng = DirectERI(build.build_basis_set(mol, basis_name), mol, device=_STATE["device"],
+                        schwarz_tau=_STATE["schwarz_tau"])
+    return _to_host(ours(mol, result, engine=eng))
+
+
 _TARGETS = [
     ("jax_qc.integrals.interface", "compute_integrals", compute_integrals),
     ("jax_qc", "compute_integrals", compute_integrals),
@@ -129,6 +152,10 @@ _TARGETS = [
     ("jax_qc.scf.uhf", "build_fock_uhf", build_fock_uhf),
     ("jax_qc.scf.guess", "core_guess_uhf", core_guess_uhf),
     ("jax_qc.scf.uhf", "core_guess_uhf", core_guess_uhf),
+    ("jax_qc.grad.rhf_grad", "rhf_gradient", rhf_gradient),
+    ("jax_qc.grad.interface", "rhf_gradient", rhf_gradient),
+    ("jax_qc.geomopt.optimizer", "rhf_gradient", rhf_gradient),
+    ("jax_qc.geomopt.hessian", "rhf_gradient", rhf_gradient),
 ]
 
 

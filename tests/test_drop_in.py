@@ -85,3 +85,18 @@ def test_reference_scf_through_drop_in(ref, golden, tag):
     res = jax_qc.run_scf(rmol, ints, CalcConfig(method="uhf" if mol.spin else "rhf", scf_conv=1e-10))
     assert fake.calls > 3
     assert abs(float(res.energy) - g.rec["energy"]) < 1e-9
+
+
+def test_gradient_and_bfgs_callers_are_rebound(ref):
+    """rhf_gradient is rebound where the reference imported it by name
+    (grad/interface.py:17, geomopt/optimizer.py:30, geomopt/hessian.py:21),
+    so the reference's BFGS and FD Hessian call the analytic gradient."""
+    jax_qc, names = ref
+    import importlib
+
+    from jax_examples_b200 import drop_in
+
+    for mod in ("jax_qc.grad.rhf_grad", "jax_qc.grad.interface", "jax_qc.geomopt.optimizer",
+                "jax_qc.geomopt.hessian"):
+        assert f"{mod}.rhf_gradient" in names
+        assert importlib.import_module(mod).rhf_gradient is drop_in.rhf_gradient

@@ -78,3 +78,19 @@ def test_uhf_gradient_vs_numerical(golden):
     grad = uhf_gradient(mol, res).cpu().numpy()
     num = numerical_gradient(mol, "syn-sto-3g", step_size=1e-4, scf_conv=1e-11, device=0).numpy()
     np.testing.assert_allclose(grad, num, atol=2e-6)
+
+
+def test_drop_in_gradient_entry_point():
+    """drop_in.rhf_gradient (the signature of rhf_grad.py:106) returns the
+    analytic gradient of the result's engine, in host arrays."""
+    from jax_examples_b200 import drop_in
+
+    mol = pb.water_cluster(2, seed=3)
+    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    ints = compute_integrals(mol, bs, device=0)
+    res = run_scf(mol, ints, CalcConfig(scf_conv=1e-10))
+    g = drop_in.rhf_gradient(mol, res, basis_name="syn-6-31g*", step_size=1e-4)
+    ref = rhf_gradient(mol, res, bs).cpu().numpy()
+    assert isinstance(g, np.ndarray) and g.shape == (6, 3)
+    np.testing.assert_allclose(g, ref, atol=1e-12, rtol=0)
+    assert abs(g.sum(axis=0)).max() < 1e-8  # translational invariance
