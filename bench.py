@@ -458,6 +458,10 @@ def run_ours(args):
         "gpu_launches": st["launches_per_jk"] * args.steps,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                      "frac": achieved / peak64, "traffic": None,
+                     "traffic_small_case": {"dram_bytes_per_launch": 1644800, "kernel": "jk_kernel<double,1,0,0,0>",
+                                            "case": "(H2O)8, ncu --set full",
+                                            "note": "L2-resident working set: DRAM bytes are the compulsory "
+                                                    "reads of pair data and D, not proportional to quartets"},
                      "kernel": "jk_kernel<double,%d,%d,%d,%d>" % best[2],
                      "peak_source": "FP64 FMA microbenchmark (jqc_fp_peak) measured in this run",
                      "fp32_peak": peak32,
