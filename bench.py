@@ -222,6 +222,76 @@ def batched_sweep(local: int, n_mol: int, seed: int = 2024):
     }
 
 
+def kernel_configs(local: int):
+    """The kernel-level configurations beside the Fock build: Boys
+    throughput (2^24 T, half U[0,30], half log-U[1e-8,1e3], m = 0..8, FP64
+    and FP32; HBM bound), primitive-quartet blocks of four classes (2^20
+    random quartets each, exponents log-U[0.1,100], centres in a 4 A cube)
+    and the (H2O)8 J/K build in 6-31G* (FP64 and mixed) and 6-31G**."""
+    import torch
+
+    from jax_examples_b200 import DirectERI, boys, eri_prim_quartets
+    from jax_examples_b200 import basis as pb
+
+    dev = torch.device("cuda", local)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    rng = np.random.default_rng(1)
+    n = 1 << 24
+    T = torch.tensor(np.concatenate([rng.uniform(0, 30, n // 2), 10 ** rng.uniform(-8, 3, n // 2)]), device=dev)
+    out = {}
+    for fp32 in (False, True):
+        sec = timed(lambda: boys(T, 8, fp32=fp32))
+        nbytes = n * 8 + n * 9 * (4 if fp32 else 8)
+        out["boys_fp32" if fp32 else "boys_fp64"] = {
+            "values_per_s": n * 9 / sec, "ms": round(sec * 1e3, 3), "gbs": nbytes / sec / 1e9,
+            "hbm_frac": nbytes / sec / 1e9 / hbm}
+    del T
+    classes = {"(ss|ss)": (0, 0, 0, 0), "(pp|pp)": (1, 1, 1, 1), "(dd|dd)": (2, 2, 2, 2), "(ds|ps)": (2, 0, 1, 0)}
+    nq = 1 << 20
+    prim = {}
+    for name, cls in classes.items():
+        ex = torch.tensor(10 ** rng.uniform(-1, 2, (nq, 4)), device=dev)
+        ctr = torch.tensor(rng.uniform(0, 4.0 / 0.529177210903, (nq, 4, 3)), device=dev)
+        sec = timed(lambda: eri_prim_quartets(cls, ex, ctr), reps=2)
+        prim[name] = {"prim_quartets_per_s": nq / sec, "ms": round(sec * 1e3, 3)}
+        del ex, ctr
+        torch.cuda.empty_cache()
+    out["prim_quartets"] = prim
+    h2o8 = {}
+    for basis in ("syn-6-31g*", "syn-6-31g**"):
+        mol = pb.water_cluster(8, seed=0)
+        bs = pb.build_basis_set(mol, basis)
+        eng = DirectERI(bs, mol, device=local, schwarz_tau=SCHWARZ_TAU)
+        D = torch.eye(bs.n_basis, dtype=torch.float64, device=dev) * 0.1
+        row = {"n_bf": bs.n_basis, "quartets": eng.stats("fp64")["quartets_fp64"]}
+        row["fp64_ms"] = round(timed(lambda: eng.jk(D)) * 1e3, 3)
+        if basis == "syn-6-31g*":
+            eng.stats("mixed", 1e-7)
+            row["mixed_ms"] = round(timed(lambda: eng.jk(D, precision="mixed", mixed_tau=1e-7)) * 1e3, 3)
+        h2o8[basis] = row
+        eng.close()
+    out["h2o8_jk"] = h2o8
+    return out
+
+
 def gradient_only(args):
     """ERI-derivative adjoint alone (the profiling case of the gradient
     kernels): core-guess density of the workload, --warmup untimed and
@@ -440,6 +510,7 @@ def run_ours(args):
     sweep = None
     if world == 1 and args.batch_molecules > 0:
         sweep = batched_sweep(local, args.batch_molecules)
+    kconf = kernel_configs(local) if (world == 1 and args.kernel_configs) else None
 
     cpu = None
     if world == 1 and not args.no_cpu:
@@ -472,6 +543,7 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "fock_gradient": fg,
         "batched_sweep": sweep,
+        "kernel_configs": kconf,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
@@ -492,6 +564,8 @@ def main():
     ap.add_argument("--batch-molecules", type=int, default=64,
                     help="molecules in the batched uneven-size sweep (0 skips it)")
     ap.add_argument("--waters", type=int, default=None, help="cluster size (default 16; profiling uses smaller)")
+    ap.add_argument("--no-kernel-configs", dest="kernel_configs", action="store_false",
+                    help="skip the Boys / primitive-quartet / (H2O)8 kernel sections")
     ap.add_argument("--gradient-only", action="store_true",
                     help="time only the ERI-derivative adjoint (profiling case)")
     args = ap.parse_args()

@@ -1322,15 +1322,20 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
     JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
     dmax = c->d_dmax.ptr;
   }
-  // per-class time of the current settings: min over two timed builds
+  // per-class time of the current settings: min over two timed builds, or
+  // one when a build takes long enough (> 30 ms) for one to be steady
   double ms[2 * kNumQuartetClasses], best_ms[kNumQuartetClasses];
   auto time_classes = [&](double* per_class) -> int {
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) per_class[qc] = 1e300;
     for (int rep = 0; rep < 2; ++rep) {
       int r = run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dens_tau, s, ms);
       if (r) return r;
-      for (int qc = 0; qc < kNumQuartetClasses; ++qc)
+      double total = 0.0;
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
         per_class[qc] = std::min(per_class[qc], ms[qc] + ms[kNumQuartetClasses + qc]);
+        total += ms[qc] + ms[kNumQuartetClasses + qc];
+      }
+      if (total > 30.0) break;
     }
     return JQC_OK;
   };

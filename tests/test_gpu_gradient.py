@@ -94,3 +94,30 @@ def test_drop_in_gradient_entry_point():
     assert isinstance(g, np.ndarray) and g.shape == (6, 3)
     np.testing.assert_allclose(g, ref, atol=1e-12, rtol=0)
     assert abs(g.sum(axis=0)).max() < 1e-8  # translational invariance
+
+
+def test_h2o16_gradient_vs_central_fd_six_coordinates():
+    """The (H2O)16 6-31G*-shaped workload: analytic gradient against finite
+    differences of SCF energies (h = 1e-4 bohr, the fourth-order central
+    stencil: the forces of this unrelaxed lattice reach 0.5 Eh/bohr, where
+    the two-point stencil's h^2 error is ~3e-6) at 6 seeded coordinates; SCF
+    converged to 1e-11 so the FD noise stays near 2e-7."""
+    mol = pb.water_cluster(16, seed=0)
+    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    cfg = CalcConfig(scf_conv=1e-11, schwarz_tau=1e-13, incremental=False)  # full FP64 builds: smooth E(R)
+    ints = compute_integrals(mol, bs, device=0, schwarz_tau=1e-13)
+    res = run_scf(mol, ints, cfg)
+    g = rhf_gradient(mol, res, bs).cpu().numpy()
+    rng = np.random.default_rng(16)
+    picks = [(int(a), int(x)) for a, x in zip(rng.integers(0, 48, 6), rng.integers(0, 3, 6))]
+    h = 1e-4
+    for a, x in picks:
+        e = {}
+        for k in (2, 1, -1, -2):
+            xyz = np.array(mol.coords, dtype=np.float64)
+            xyz[a, x] += k * h
+            m2 = make_molecule(mol.elements, xyz, np.asarray(mol.atomic_numbers))
+            b2 = pb.build_basis_set(m2, "syn-6-31g*")
+            e[k] = run_scf(m2, compute_integrals(m2, b2, device=0, schwarz_tau=1e-13), cfg).energy
+        fd = (8.0 * (e[1] - e[-1]) - (e[2] - e[-2])) / (12.0 * h)
+        assert abs(fd - g[a, x]) < 1e-6, (a, x, fd, g[a, x])
