@@ -894,11 +894,10 @@ int jqc_boys(const double* T, long long n, int mmax, void* out, int fp32, void* 
   JQC_REQUIRE(T && out, JQC_ERR_INVALID, "jqc_boys: null pointer");
   int dev = 0;
   JQC_CUDA_CHECK(cudaGetDevice(&dev));
-  const double* t64;
-  const float* t32;
-  int rc = boys_tables(dev, &t64, &t32);
+  BoysTables bt;
+  int rc = boys_tables_all(dev, &bt);
   if (rc) return rc;
-  JQC_CUDA_CHECK(launch_boys(T, n, mmax, out, fp32 != 0, fp32 ? (const void*)t32 : (const void*)t64,
+  JQC_CUDA_CHECK(launch_boys(T, n, mmax, out, fp32 != 0, fp32 ? (const void*)bt.a32 : (const void*)bt.a64,
                              static_cast<cudaStream_t>(stream)));
   return JQC_OK;
 }

@@ -124,7 +124,7 @@ cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuart
   const int pb = pair_class(la, lb), pk = pair_class(lc, ld);
   if (pb < pk) return cudaErrorInvalidValue;
   const unsigned gx = (unsigned)((p.n + 127) / 128);
-  if (!is_reg_class(quartet_class(pb, pk))) return launch_warp_prim(la, lb, lc, ld, p, s);
+  if (!is_reg_class(quartet_class(pb, pk))) return launch_col_prim(quartet_class(pb, pk), p, s);
   switch (quartet_class(pb, pk)) {
 #define X(Q, A, B, C, D)                                                                     \
   case Q: {                                                                                  \
@@ -140,30 +140,54 @@ cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuart
 }
 
 // -------------------------------------------------------------------- Boys
-template <typename T>
-__global__ void boys_kernel(const double* __restrict__ tv, long long n, int mmax, T* __restrict__ out,
-                            const T* __restrict__ tab) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double t = tv[i];
-  if (!(t >= 0.0)) {  // negative or NaN argument: no table access
-    for (int m = 0; m <= mmax; ++m) out[i * (mmax + 1) + m] = T(NAN);
-    return;
+// One thread per argument, the order fixed at compile time (the aligned
+// per-order table and an unrolled recursion); the block's outputs are staged
+// in shared memory and written back as one contiguous, coalesced run.
+template <typename T, int M>
+__global__ void __launch_bounds__(256) boys_kernel(const double* __restrict__ tv, long long n, T* __restrict__ out,
+                                                   const T* __restrict__ tabA) {
+  __shared__ T stage[256 * (M + 1)];
+  const long long base = (long long)blockIdx.x * 256;
+  const long long i = base + threadIdx.x;
+  if (i < n) {
+    const double t = tv[i];
+    T F[M + 1];
+    if (t >= 0.0) {
+      boys_eval<T, M>(T(t), tabA, F);
+    } else {  // negative or NaN argument: no table access
+#pragma unroll
+      for (int m = 0; m <= M; ++m) F[m] = T(NAN);
+    }
+#pragma unroll
+    for (int m = 0; m <= M; ++m) stage[threadIdx.x * (M + 1) + m] = F[m];
   }
-  T F[kBoysMaxM + 1];
-  boys_eval_rt<T>(T(t), tab, mmax, F);
-  for (int m = 0; m <= mmax; ++m) out[i * (mmax + 1) + m] = F[m];
+  __syncthreads();
+  const long long cnt = (n - base < 256 ? n - base : 256) * (M + 1);
+  T* dst = out + base * (M + 1);
+  for (long long k = threadIdx.x; k < cnt; k += 256) dst[k] = stage[k];
 }
 
-cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tab,
+template <typename T>
+static cudaError_t launch_boys_t(const double* tv, long long n, int mmax, T* out, const T* tabA, cudaStream_t s) {
+  const unsigned g = (unsigned)((n + 255) / 256);
+  switch (mmax) {
+#define B(Mv)                                                   \
+  case Mv:                                                      \
+    boys_kernel<T, Mv><<<g, 256, 0, s>>>(tv, n, out, tabA);     \
+    break;
+    B(0) B(1) B(2) B(3) B(4) B(5) B(6) B(7) B(8) B(9) B(10) B(11) B(12) B(13) B(14) B(15) B(16)
+#undef B
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tabA,
                         cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  const unsigned g = (unsigned)((n + 255) / 256);
-  if (fp32)
-    boys_kernel<float><<<g, 256, 0, s>>>(T, n, mmax, static_cast<float*>(out), static_cast<const float*>(tab));
-  else
-    boys_kernel<double><<<g, 256, 0, s>>>(T, n, mmax, static_cast<double*>(out), static_cast<const double*>(tab));
-  return cudaGetLastError();
+  if (fp32) return launch_boys_t<float>(T, n, mmax, static_cast<float*>(out), static_cast<const float*>(tabA), s);
+  return launch_boys_t<double>(T, n, mmax, static_cast<double*>(out), static_cast<const double*>(tabA), s);
 }
 
 // --------------------------------------------------------------- helpers

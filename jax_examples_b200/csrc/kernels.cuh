@@ -80,7 +80,8 @@ cudaError_t launch_jk(int qc, bool fp32, const JKParams& p, cudaStream_t s);
 cudaError_t launch_eri_tensor(int qc, const TensorParams& p, cudaStream_t s);
 cudaError_t launch_schwarz(int pc, const SchwarzParams& p, cudaStream_t s);
 cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s);
-cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tab, cudaStream_t s);
+// tabA: the aligned per-order Boys table of the output type.
+cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tabA, cudaStream_t s);
 cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
                         cudaStream_t s);
 cudaError_t launch_symmetrize(double* M, int count, int n, cudaStream_t s);
@@ -170,6 +171,7 @@ cudaError_t launch_pair_force_reduce(const ShellPair* pairs, int n_pairs, const 
 cudaError_t launch_warp_jk(int la, int lb, int lc, int ld, bool fp32, const JKParams& p, cudaStream_t s);
 bool has_col_class(int qc);
 cudaError_t launch_col_jk(int qc, bool fp32, const JKParams& p, cudaStream_t s);
+cudaError_t launch_col_prim(int qc, const PrimQuartetParams& p, cudaStream_t s);  // classes 19, 20
 
 cudaError_t launch_warp_tensor(int la, int lb, int lc, int ld, const TensorParams& p, cudaStream_t s);
 cudaError_t launch_warp_schwarz(int la, int lb, const SchwarzParams& p, cudaStream_t s);
