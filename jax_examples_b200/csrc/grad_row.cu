@@ -132,23 +132,33 @@ __device__ __noinline__ F6 row_bra(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
     dby[t] = sm->DB[1][ay][by][t];
     dbz[t] = sm->DB[2][az][bz][t];
   });
-  F6 out = {{0, 0, 0, 0, 0, 0}};
+  // Z[h] = sum_k Fg[k] R_{h+k}: k outer, so the NH1 sums are independent
+  double Z[NH1];
+  static_for<NH1>([&](auto h_) { Z[decltype(h_)::value] = 0.0; });
+  static_for<NK0>([&](auto k_) {
+    constexpr int k = decltype(k_)::value;
+    const double f = Fg[k];
+    static_for<NH1>([&](auto h_) {
+      constexpr int h = decltype(h_)::value;
+      Z[h] += f * sm->R[herm_index(gr_ht(h) + gr_ht(k), gr_hu(h) + gr_hu(k), gr_hv(h) + gr_hv(k))];
+    });
+  });
+  // two partial sums per component (even / odd h) halve the dependency chains
+  double acc[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
   static_for<NH1>([&](auto h_) {
     constexpr int h = decltype(h_)::value;
-    constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h);
-    double z = 0.0;
-    static_for<NK0>([&](auto k_) {
-      constexpr int k = decltype(k_)::value;
-      constexpr int ri = herm_index(t + gr_ht(k), u + gr_hu(k), v + gr_hv(k));
-      z += Fg[k] * sm->R[ri];
-    });
-    out.v[0] += dax[t] * ey[u] * ez[v] * z;
-    out.v[1] += ex[t] * day[u] * ez[v] * z;
-    out.v[2] += ex[t] * ey[u] * daz[v] * z;
-    out.v[3] += dbx[t] * ey[u] * ez[v] * z;
-    out.v[4] += ex[t] * dby[u] * ez[v] * z;
-    out.v[5] += ex[t] * ey[u] * dbz[v] * z;
+    constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h), q = h & 1;
+    const double z = Z[h];
+    acc[q][0] += dax[t] * ey[u] * ez[v] * z;
+    acc[q][1] += ex[t] * day[u] * ez[v] * z;
+    acc[q][2] += ex[t] * ey[u] * daz[v] * z;
+    acc[q][3] += dbx[t] * ey[u] * ez[v] * z;
+    acc[q][4] += ex[t] * dby[u] * ez[v] * z;
+    acc[q][5] += ex[t] * ey[u] * dbz[v] * z;
   });
+  F6 out;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) out.v[k] = acc[0][k] + acc[1][k];
   return out;
 }
 
@@ -177,16 +187,16 @@ __device__ __noinline__ F3 row_ket(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
       Gab[h] = ex[gr_ht(h)] * ey[gr_hu(h)] * ez[gr_hv(h)];
     });
   }
+  // W[k] = sum_h Gab[h] R_{h+k}: h outer, so the NK1 sums are independent
   double W[NK1];
-  static_for<NK1>([&](auto k_) {
-    constexpr int k = decltype(k_)::value;
-    constexpr int tk = gr_ht(k), uk = gr_hu(k), vk = gr_hv(k);
-    double w = 0.0;
-    static_for<NH0>([&](auto h_) {
-      constexpr int h = decltype(h_)::value;
-      w += Gab[h] * sm->R[herm_index(gr_ht(h) + tk, gr_hu(h) + uk, gr_hv(h) + vk)];
+  static_for<NK1>([&](auto k_) { W[decltype(k_)::value] = 0.0; });
+  static_for<NH0>([&](auto h_) {
+    constexpr int h = decltype(h_)::value;
+    const double gh = Gab[h];
+    static_for<NK1>([&](auto k_) {
+      constexpr int k = decltype(k_)::value;
+      W[k] += gh * sm->R[herm_index(gr_ht(h) + gr_ht(k), gr_hu(h) + gr_hu(k), gr_hv(h) + gr_hv(k))];
     });
-    W[k] = w;
   });
   F3 out = {{0, 0, 0}};
   static_for<NCD>([&](auto cd_) {
@@ -221,8 +231,16 @@ __device__ __noinline__ F3 row_ket(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
   return out;
 }
 
+// Resident blocks per SM the register allocation aims at: 3 (<= 168
+// registers, a few KB of spills) pays for the dp bras and (dd|ps); the other
+// dd-bra classes are limited by shared memory anyway and lose to the spills.
+__host__ __device__ constexpr int grad_row_min_blocks(int la, int lb, int lc, int ld) {
+  return (lb == 1 || (lb == 2 && lc == 1 && ld == 0)) ? 3 : 1;
+}
+
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(32 * kGRowWarps) grad_row_kernel(const GradParams prm) {
+__global__ void __launch_bounds__(32 * kGRowWarps, grad_row_min_blocks(LA, LB, LC, LD))
+    grad_row_kernel(const GradParams prm) {
   using S = GRowSmem<LA, LB, LC, LD>;
   constexpr int LAB = S::LAB, LCD = S::LCD, L = S::L, NAB = S::NAB, NCD = S::NCD;
   constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
