@@ -18,7 +18,7 @@ namespace jqc {
 __host__ __device__ constexpr int grad_split(int la, int lb, int lc, int ld) {
   int nab = ncart(la) * ncart(lb), ncd = ncart(lc) * ncart(ld);
   int ns = 1;
-  while (ns < 16 && nab * ((ncd + ns - 1) / ns) > 18 && ns < ncd) ns *= 2;
+  while (ns < 16 && nab * ((ncd + ns - 1) / ns) > 9 && ns < ncd) ns *= 2;
   return ns;
 }
 
