@@ -155,7 +155,7 @@ class CalcConfig(_Replace):
     fp64_tail_iters: int = 2
     fp64_switch: float = 1e-5
     incremental: bool = True
-    mixed_dens_tau: float = 1e-9
+    mixed_dens_tau: float = 1e-8
 
 
 def make_molecule(elements, coords, atomic_numbers, charge: int = 0, spin: int = 0) -> Molecule:

@@ -198,7 +198,7 @@ __device__ __forceinline__ void prim_quartet_R(const PPT& bp, const PPT& kp, con
 
 // Classes whose bra angular sum is at most this loop over ket primitives
 // outermost (see quartet_accumulate).
-constexpr int kKetOuterMaxLab = 1;
+constexpr int kKetOuterMaxLab = 2;
 
 // Accumulates the contracted block (ab|cd) for the ket Cartesian pairs of
 // part PART into out[ab][cdi] (cd = CD0 + cdi).  Loops over all primitive

@@ -13,9 +13,9 @@ the precision policy of the mixed path:
   the density change dD = D - D_prev (J, K are linear in D) with density-
   weighted screening, the error of which is reset by a full rebuild every
   ``rebuild_every`` builds.  In this phase the incremental builds screen at
-  ``mixed_dens_tau`` (1e-9: the early Fock matrices only steer the next
-  density; a threshold that follows the DIIS error upward of that slowed the
-  convergence more than it saved).  When the SCF error
+  ``mixed_dens_tau`` (1e-8: the early Fock matrices only steer the next
+  density; 3e-8 and a threshold that follows the DIIS error upward already
+  cost more iterations than they save).  When the SCF error
   drops below ``fp64_switch`` the builder switches to FP64 with a full
   rebuild and then tight-threshold incremental FP64 builds, and convergence
   is only accepted after ``fp64_tail_iters`` of them: the final energy is an
@@ -100,7 +100,7 @@ class FockBuilder:
         self.fp64_switch = float(getattr(config, "fp64_switch", 1e-5))
         self.rebuild_every = rebuild_every
         self.dens_tau = dens_tau
-        self.mixed_dens_tau = float(getattr(config, "mixed_dens_tau", 1e-9))
+        self.mixed_dens_tau = float(getattr(config, "mixed_dens_tau", 1e-8))
         self.phase = "mixed" if (self.precision == "mixed" and self.direct) else "fp64"
         self.fp64_builds_after_switch = 0
         self.switched = self.phase == "fp64"
