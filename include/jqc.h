@@ -216,8 +216,9 @@ int jqc_set_grad_engine(jqc_ctx *ctx, int quartet_class, int engine);
 int jqc_get_grad_engine(jqc_ctx *ctx, int *engines21);
 
 /* Autotuner: times every class of the J/K build for this density, precision
- * and screening (classes serialised, CUDA events, best of two) over the
- * engines, then threads x persistent, then lane_prims, keeps the fastest
+ * and screening (classes serialised, CUDA events, best of two, or one when a
+ * build takes over 30 ms) over the engines, then threads (128, 256) x
+ * persistent, then lane_prims (64, 128, 256, 512), keeps the fastest
  * shape per class and rebuilds the work list with it.  With cache_path, a
  * line "signature<TAB>84 integers" is appended; a later call whose signature
  * (device, settings, order of magnitude of each class's quartet count)

@@ -1369,8 +1369,8 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
   rc = rebuild();
   if (rc) return rc;
   // 3. block size and grid form of the register kernels (no rebuild needed)
-  const int th_opts[3] = {64, 128, 256};
-  for (int ti = 0; ti < 3; ++ti)
+  const int th_opts[2] = {128, 256};
+  for (int ti = 0; ti < 2; ++ti)
     for (int pe = 0; pe < 2; ++pe) {
       for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
         c->tune[qc].threads = th_opts[ti];
@@ -1386,12 +1386,12 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
         }
     }
   // 4. bra primitive chunk (work list rebuilt per value)
-  const int lp_opts[4] = {64, 128, 512, 1024};
+  const int lp_opts[3] = {64, 128, 512};
   for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
     c->tune[qc].threads = best[qc].threads;
     c->tune[qc].persistent = best[qc].persistent;
   }
-  for (int li = 0; li < 4; ++li) {
+  for (int li = 0; li < 3; ++li) {
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) c->tune[qc].lane_prims = lp_opts[li];
     rc = rebuild();
     if (rc) return rc;

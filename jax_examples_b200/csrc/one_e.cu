@@ -34,8 +34,11 @@ struct OneEParams {
   double* V;
 };
 
+// One warp per shell pair: the lanes split the nuclei of V; lane 0 adds the
+// overlap and kinetic terms; the three blocks are reduced over the warp.
 __global__ void one_e_kernel(const OneEParams p) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   const int npair = p.n_shell * (p.n_shell + 1) / 2;
   if (idx >= npair) return;
   int i = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
@@ -98,18 +101,19 @@ __global__ void one_e_kernel(const OneEParams p) {
             T1[x][a][b] = 0.5 * tv;
           }
       }
-      for (int a = 0; a < na; ++a)
-        for (int b = 0; b < nb; ++b) {
-          int ax, ay, az, bx, by, bz;
-          wcart(la, a, ax, ay, az);
-          wcart(lb, b, bx, by, bz);
-          const double sx = S1[0][ax][bx], sy = S1[1][ay][by], sz = S1[2][az][bz];
-          s[a * nb + b] += K * sx * sy * sz;
-          t[a * nb + b] += K * (T1[0][ax][bx] * sy * sz + sx * T1[1][ay][by] * sz + sx * sy * T1[2][az][bz]);
-        }
-      // nuclear attraction
+      if (lane == 0)
+        for (int a = 0; a < na; ++a)
+          for (int b = 0; b < nb; ++b) {
+            int ax, ay, az, bx, by, bz;
+            wcart(la, a, ax, ay, az);
+            wcart(lb, b, bx, by, bz);
+            const double sx = S1[0][ax][bx], sy = S1[1][ay][by], sz = S1[2][az][bz];
+            s[a * nb + b] += K * sx * sy * sz;
+            t[a * nb + b] += K * (T1[0][ax][bx] * sy * sz + sx * T1[1][ay][by] * sz + sx * sy * T1[2][az][bz]);
+          }
+      // nuclear attraction, nuclei split over the lanes
       const int L = la + lb;
-      for (int c = 0; c < p.n_atom; ++c) {
+      for (int c = lane; c < p.n_atom; c += 32) {
         if (p.atom_mol && p.atom_mol[c] != mol) continue;  // nuclei of this molecule only
         const double X = P[0] - p.atom_xyz[3 * c], Y = P[1] - p.atom_xyz[3 * c + 1], Z = P[2] - p.atom_xyz[3 * c + 2];
         double F[kBoysMaxM + 1];
@@ -159,6 +163,13 @@ __global__ void one_e_kernel(const OneEParams p) {
           }
       }
     }
+  for (int x = 0; x < na * nb; ++x) {
+    double vx = v[x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vx += __shfl_xor_sync(0xffffffffu, vx, o);
+    v[x] = vx;
+  }
+  if (lane != 0) return;
   const int a0 = p.ao[i], b0 = p.ao[j];
   for (int a = 0; a < na; ++a)
     for (int b = 0; b < nb; ++b) {
@@ -170,9 +181,9 @@ __global__ void one_e_kernel(const OneEParams p) {
 }
 
 cudaError_t launch_one_e(const OneEParams& p, cudaStream_t s) {
-  const int npair = p.n_shell * (p.n_shell + 1) / 2;
+  const long long npair = (long long)p.n_shell * (p.n_shell + 1) / 2;
   if (npair == 0) return cudaSuccess;
-  one_e_kernel<<<(npair + 127) / 128, 128, 0, s>>>(p);
+  one_e_kernel<<<(unsigned)((npair * 32 + 127) / 128), 128, 0, s>>>(p);
   return cudaGetLastError();
 }
 
