@@ -164,7 +164,7 @@ def batched_sweep(local: int, n_mol: int, seed: int = 2024):
 
     from jax_examples_b200 import CalcConfig, DirectERI, compute_integrals, run_scf
     from jax_examples_b200 import basis as pb
-    from jax_examples_b200.batch import MIXED_GRAD_TAU, MoleculeBatch, rhf_gradient_batch, run_rhf_batch
+    from jax_examples_b200.batch import MIXED_GRAD_TAU, BatchedERI, MoleculeBatch, rhf_gradient_batch, run_rhf_batch
     from jax_examples_b200.grad import rhf_gradient
 
     rng = np.random.default_rng(seed)
@@ -175,7 +175,11 @@ def batched_sweep(local: int, n_mol: int, seed: int = 2024):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     batch = MoleculeBatch(mols, BASIS)
-    scf = run_rhf_batch(batch, chosen, use_graph=True, autotune=True)
+    t_ctx = time.perf_counter()
+    beng = BatchedERI(batch, schwarz_tau=SCHWARZ_TAU)
+    torch.cuda.synchronize()
+    t_ctx = time.perf_counter() - t_ctx
+    scf = run_rhf_batch(batch, chosen, engine=beng, use_graph=True, autotune=True)
     timing = {}
     grads = rhf_gradient_batch(batch, scf, timing, MIXED_GRAD_TAU)
     torch.cuda.synchronize()
@@ -212,6 +216,8 @@ def batched_sweep(local: int, n_mol: int, seed: int = 2024):
                           "fock_builds": rec["fock_builds"],
                           "builds": {k: rec[k] for k in ("builds_mixed", "builds_fp64", "incremental_builds")},
                           "gradient_dens_tau": MIXED_GRAD_TAU, "setup_s": round(rec["setup_seconds"], 3),
+                          "setup_breakdown_s": dict({k: round(v, 3) for k, v in rec["prepare_breakdown"].items()},
+                                                    context_pairs=round(t_ctx, 3)),
                           "wall_s": round(t_batch, 3), "graph": rec["graph"], "autotuned": rec["autotuned"]},
         "sequential_fp64": {"fock_s": round(fock_seq, 4), "gradient_s": round(grad_seq, 4),
                             "iterations_mean": float(np.mean(iters)), "wall_s": round(t_seq, 3)},

@@ -39,7 +39,6 @@ from .core import BasisSet, CalcConfig, SCFResult, SCFState, Shell, make_molecul
 from .engine import DirectERI, _ptr, _stream
 from .grad import energy_weighted_density, grad_one_electron, grad_two_electron, nuclear_repulsion_gradient
 from .integrals import nuclear_repulsion_energy
-from .scf import DIIS, diis_error, symmetric_orthogonalization
 
 # Density-screening threshold of the batched FP64 builds.  A quartet is
 # skipped only when Q_ab Q_cd max|D| < 1e-30, i.e. when its density blocks are
@@ -238,22 +237,6 @@ class BatchedERI:
 # lock-step RHF
 # ---------------------------------------------------------------------------
 
-def _diag_groups(F_list, X_list, idx):
-    """eps, C of X^T F X for the molecules idx, one batched eigh per size."""
-    out = {}
-    by_n = {}
-    for m in idx:
-        by_n.setdefault(X_list[m].shape[0], []).append(m)
-    for _, ms in by_n.items():
-        X = torch.stack([X_list[m] for m in ms])
-        F = torch.stack([F_list[m] for m in ms])
-        e, V = torch.linalg.eigh(X.transpose(1, 2) @ F @ X)
-        C = X @ V
-        for i, m in enumerate(ms):
-            out[m] = (e[i], C[i])
-    return out
-
-
 class BatchSCF(NamedTuple):
     """Per-molecule SCF results of a batch and the batch's build record."""
 
@@ -329,16 +312,22 @@ class _BatchFock:
         for m, d in dens.items():
             self.batch.block(self.D[0], m).copy_(d)
         prec, tau = self._settings(False)
+        self.prep_times = {}
         if autotune:
+            t0 = time.perf_counter()
             self.eng.autotune(self.D, self.J, self.K, prec, self.mixed_tau, tau, cache_path=tune_cache)
+            self.prep_times["autotune"] = time.perf_counter() - t0
         if self.use_graph:
             kinds = [(prec, tau)]
             if self.mixed:
                 kinds += [("fp64", BATCH_DENS_TAU)]
             if self.incremental:
                 kinds += [("mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU)), ("fp64", 1e-12)]
+            t0 = time.perf_counter()
             for p_, t_ in kinds:
                 self.graphs[(p_, t_)] = self.eng.capture_jk(self.D, self.J, self.K, p_, self.mixed_tau, t_)
+            torch.cuda.synchronize()
+            self.prep_times["capture"] = time.perf_counter() - t0
 
     def build(self, dens: dict) -> dict:
         """(J_m, K_m) of the molecules in dens."""
@@ -395,6 +384,54 @@ class _BatchFock:
         return sum(a.elapsed_time(c) for a, c in self.events) * 1e-3
 
 
+class _Group:
+    """Molecules of one (basis size, occupied count): their SCF state as
+    stacked (G, n, n) tensors, so every step of the iteration is one batched
+    operation per group."""
+
+    def __init__(self, members, S, H, n_occ):
+        self.members = list(members)
+        self.S, self.H = S, H
+        self.n_occ = n_occ
+        w, U = torch.linalg.eigh(S)
+        self.X = (U * (1.0 / torch.sqrt(w))[:, None, :]) @ U.transpose(1, 2)  # S^-1/2 (orthogonalize.py:22-26)
+        self.Fh, self.Eh = [], []  # DIIS history, oldest first
+
+    def diag(self, F):
+        e, V = torch.linalg.eigh(self.X.transpose(1, 2) @ F @ self.X)
+        return e, self.X @ V
+
+    def density(self, C):
+        Co = C[:, :, :self.n_occ]
+        return 2.0 * Co @ Co.transpose(1, 2)
+
+    def diis(self, F, err, size: int):
+        """Pulay extrapolation of every member (diis.py:53-130): ring buffer of
+        ``size`` pairs, B_ij = <e_i, e_j> bordered by -1, fallback to F when
+        the system is singular or the history has fewer than two entries."""
+        self.Fh.append(F)
+        self.Eh.append(err)
+        if len(self.Fh) > size:
+            self.Fh.pop(0)
+            self.Eh.pop(0)
+        m = len(self.Fh)
+        if m < 2:
+            return F
+        G = F.shape[0]
+        E = torch.stack(self.Eh, 1).reshape(G, m, -1)
+        B = torch.empty((G, m + 1, m + 1), dtype=F.dtype, device=F.device)
+        B[:, :m, :m] = E @ E.transpose(1, 2)
+        B[:, m, :m] = -1.0
+        B[:, :m, m] = -1.0
+        B[:, m, m] = 0.0
+        rhs = torch.zeros((G, m + 1, 1), dtype=F.dtype, device=F.device)
+        rhs[:, m, 0] = -1.0
+        c, info = torch.linalg.solve_ex(B, rhs)
+        Fx = torch.einsum("gi,gimn->gmn", c[:, :m, 0], torch.stack(self.Fh, 1))
+        ok = (info == 0) & torch.isfinite(c[:, :m, 0]).all(dim=1)
+        return torch.where(ok[:, None, None], Fx, F)
+
+
 def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, engine: Optional[BatchedERI] = None,
                   use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None) -> BatchSCF:
     """Closed-shell SCF of every molecule of the batch, in lock step.
@@ -404,8 +441,11 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     X = S^-1/2, F0 from the guess density, DIIS, converged when
     dE < scf_conv and max|DIIS error| < max(scf_conv, 1e-6).  All molecules
     share each Fock build (one graph replay of the batch J/K, see
-    :class:`_BatchFock` for the precision policy of ``config.precision``); a
-    converged molecule keeps its state and leaves the builds.
+    :class:`_BatchFock` for the precision policy of ``config.precision``); the
+    rest of an iteration (DIIS error, extrapolation, eigh, density, energy)
+    runs as batched tensor operations per group of equal-size molecules with
+    one host read per iteration.  A converged molecule keeps its state and
+    leaves the builds.
     """
     config = config or CalcConfig()
     for mol in batch.mols:
@@ -416,73 +456,99 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     t_setup = time.perf_counter()
     S_all, T_all, V_all = eng.engine.one_electron()
     H_all = T_all + V_all
-    S = [batch.block(S_all, m).clone() for m in range(M)]
-    H = [batch.block(H_all, m).clone() for m in range(M)]
-    X = [symmetric_orthogonalization(s) for s in S]
     n_occ = [mol.n_electrons // 2 for mol in batch.mols]
     E_nuc = [nuclear_repulsion_energy(mol) for mol in batch.mols]
+    keys = {}
+    for m in range(M):
+        keys.setdefault((batch.n_bf[m], n_occ[m]), []).append(m)
+    groups = []
+    for (n, no), members in keys.items():
+        S = torch.stack([batch.block(S_all, m) for m in members])
+        H = torch.stack([batch.block(H_all, m) for m in members])
+        groups.append(_Group(members, S, H, no))
     fb = _BatchFock(eng, batch, config, use_graph)
 
-    def fock(dens: dict) -> dict:
-        jk = fb.build(dens)
-        return {m: H[m] + jk[m][0] - 0.5 * jk[m][1] for m in dens}
+    def fock(g: _Group, jk: dict, fallback):
+        J = torch.stack([jk[m][0] if m in jk else fallback[i] * 0 for i, m in enumerate(g.members)])
+        K = torch.stack([jk[m][1] if m in jk else fallback[i] * 0 for i, m in enumerate(g.members)])
+        return g.H + J - 0.5 * K
 
     # core guess (rhf.py:111-121)
-    all_m = list(range(M))
-    dg = _diag_groups(H, X, all_m)
-    D = {m: 2.0 * dg[m][1][:, :n_occ[m]] @ dg[m][1][:, :n_occ[m]].T for m in all_m}
-    fb.prepare(D, autotune, tune_cache)
+    for g in groups:
+        _, C = g.diag(g.H)
+        g.D = g.density(C)
+    dens = {m: g.D[i] for g in groups for i, m in enumerate(g.members)}
+    torch.cuda.synchronize()
+    t_prep = time.perf_counter()
+    fb.prepare(dens, autotune, tune_cache)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
-    F = fock(D)
-    dg = _diag_groups(F, X, all_m)
-    eps = {m: dg[m][0] for m in all_m}
-    C = {m: dg[m][1] for m in all_m}
-    E = torch.stack([0.5 * torch.sum(D[m] * (H[m] + F[m])) for m in all_m]).cpu().numpy()
-    last = E.copy()
-    diis = [DIIS(config.diis_space) for _ in all_m]
-    iters = [0] * M
-    converged = [False] * M
-    active = list(all_m)
+    prepare_s = time.perf_counter() - t_prep
+    jk = fb.build(dens)
+    for g in groups:
+        g.F = fock(g, jk, g.D)
+        g.eps, g.C = g.diag(g.F)
+        g.E = 0.5 * torch.sum(g.D * (g.H + g.F), dim=(1, 2))
+        g.active = torch.ones(len(g.members), dtype=torch.bool, device=g.D.device)
+        g.iters = torch.zeros(len(g.members), dtype=torch.int64, device=g.D.device)
+    last = torch.cat([g.E for g in groups]).cpu().numpy()
+    order = [m for g in groups for m in g.members]
+    pos = {m: k for k, m in enumerate(order)}
+    converged = np.zeros(M, dtype=bool)
     for _ in range(config.max_scf_iter):
-        if not active:
+        if converged.all():
             break
-        Fn = fock({m: D[m] for m in active})
-        if config.damping > 0.0:
-            Fn = {m: (1.0 - config.damping) * Fn[m] + config.damping * F[m] for m in active}
-        err = {m: diis_error(Fn[m], D[m], S[m], X[m]) for m in active}
-        Fx = {m: diis[m].extrapolate(Fn[m], err[m]) for m in active}
-        dg = _diag_groups(Fx, X, active)
-        for m in active:
-            eps[m], C[m] = dg[m]
-            D[m] = 2.0 * C[m][:, :n_occ[m]] @ C[m][:, :n_occ[m]].T
-            F[m] = Fx[m]
-            iters[m] += 1
-        En = torch.stack([0.5 * torch.sum(D[m] * (H[m] + Fx[m])) for m in active]).cpu().numpy()
-        emax = torch.stack([torch.max(torch.abs(err[m])) for m in active]).cpu().numpy()
-        fb.observe(float(emax.max()))
+        dens = {m: g.D[i] for g in groups for i, m in enumerate(g.members) if not converged[m]}
+        jk = fb.build(dens)
+        Es, emaxs = [], []
+        for g in groups:
+            act = g.active
+            Fn = fock(g, jk, g.D)
+            if config.damping > 0.0:
+                Fn = (1.0 - config.damping) * Fn + config.damping * g.F
+            err = g.X.transpose(1, 2) @ (Fn @ g.D @ g.S - g.S @ g.D @ Fn) @ g.X  # diis.py:53-59
+            Fx = g.diis(Fn, err, config.diis_space)
+            eps, C = g.diag(Fx)
+            D = g.density(C)
+            E = 0.5 * torch.sum(D * (g.H + Fx), dim=(1, 2))
+            a3 = act[:, None, None]
+            g.D = torch.where(a3, D, g.D)
+            g.F = torch.where(a3, Fx, g.F)
+            g.C = torch.where(a3, C, g.C)
+            g.eps = torch.where(act[:, None], eps, g.eps)
+            g.E = torch.where(act, E, g.E)
+            g.iters = g.iters + act.to(torch.int64)
+            Es.append(g.E)
+            emaxs.append(torch.amax(torch.abs(err), dim=(1, 2)))
+        host = torch.cat([torch.cat(Es), torch.cat(emaxs)]).cpu().numpy()
+        E_now, emax = host[:len(order)], host[len(order):]
+        act_host = ~converged[order]
+        fb.observe(float(emax[act_host].max()) if act_host.any() else 0.0)
         ok = fb.converged_ok()
-        still = []
-        for i, m in enumerate(active):
-            E[m] = En[i]
-            dE = abs(E[m] - last[m])
-            last[m] = E[m]
-            if ok and dE < config.scf_conv and emax[i] < max(config.scf_conv, 1e-6):
+        for k, m in enumerate(order):
+            if converged[m]:
+                continue
+            dE = abs(E_now[k] - last[k])
+            last[k] = E_now[k]
+            if ok and dE < config.scf_conv and emax[k] < max(config.scf_conv, 1e-6):
                 converged[m] = True
-            else:
-                still.append(m)
-        active = still
+        for g in groups:
+            g.active = torch.tensor([not converged[m] for m in g.members], device=g.D.device)
     record = dict(fb.log, fock_builds=sum(fb.log[k] for k in ("builds_mixed", "builds_fp64")),
                   jk_seconds=fb.seconds(), setup_seconds=setup_s, graph=bool(fb.graphs), autotuned=bool(autotune),
                   n_molecules=M, n_basis=batch.n_basis, precision=config.precision,
-                  incremental=fb.incremental)
-    results = []
-    for m in all_m:
-        st = SCFState(density=D[m], fock=F[m], coefficients=C[m], orbital_energies=eps[m], energy=float(E[m]),
-                      iteration=iters[m])
-        results.append(SCFResult(converged=converged[m], state=st, energy=float(E[m]) + E_nuc[m],
-                                 E_elec=float(E[m]), E_nuc=E_nuc[m], n_iterations=iters[m], S=S[m], H_core=H[m],
-                                 ERI=None, precision={"precision": config.precision, "batched": True}))
+                  incremental=fb.incremental, groups=len(groups), prepare_seconds=prepare_s,
+                  prepare_breakdown=getattr(fb, "prep_times", {}))
+    results = [None] * M
+    for g in groups:
+        iters = g.iters.cpu().numpy()
+        for i, m in enumerate(g.members):
+            e = float(g.E[i])
+            st = SCFState(density=g.D[i], fock=g.F[i], coefficients=g.C[i], orbital_energies=g.eps[i], energy=e,
+                          iteration=int(iters[i]))
+            results[m] = SCFResult(converged=bool(converged[m]), state=st, energy=e + E_nuc[m], E_elec=e,
+                                   E_nuc=E_nuc[m], n_iterations=int(iters[i]), S=g.S[i], H_core=g.H[i], ERI=None,
+                                   precision={"precision": config.precision, "batched": True})
     return BatchSCF(results=results, engine=eng, record=record)
 
 

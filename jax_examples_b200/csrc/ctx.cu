@@ -8,6 +8,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -314,58 +315,106 @@ static int prefix_count(const std::vector<ShellPair>& pairs, int start, int limi
   return lo;
 }
 
-static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s,
-                       bool grad = false) {
+// Tasks and counters of the bra pairs [g0, g1) (one worker of build_tasks).
+struct TaskPart {
   std::vector<Task> lists[2][kNumQuartetClasses];
   long long nq[2] = {0, 0}, npq = 0;
   long long cq[2][kNumQuartetClasses] = {}, cp[2][kNumQuartetClasses] = {};
+};
+
+static void build_task_part(const jqc_ctx* c, TaskPart& out, int g0, int g1, const std::vector<int>& block_of,
+                            const std::vector<std::vector<int>>& mol_blocks, int mode, double mixed_tau, bool full,
+                            bool grad) {
   const double tau = full ? 0.0 : c->tau;
+  for (int gi = g0; gi < g1; ++gi) {
+    const size_t cb = (size_t)block_of[gi];
+    const Block& B = c->blocks[cb];
+    const int pi = gi - B.start;
+    const double Qi = c->pairs[gi].Q;
+    for (const int ckb : mol_blocks[B.mol]) {
+      const size_t ck = (size_t)ckb;
+      if (ck > cb) break;
+      const Block& K = c->blocks[ck];
+      const int limit = (ck == cb) ? pi + 1 : K.count;
+      const int n_all = prefix_count(c->pairs, K.start, limit, Qi, tau);
+      int n64 = n_all;
+      if (mode == JQC_PREC_FP32) n64 = 0;
+      if (mode == JQC_PREC_MIXED) n64 = std::min(n_all, prefix_count(c->pairs, K.start, limit, Qi, mixed_tau));
+      const int qc = quartet_class(B.pc, K.pc);
+      const int seg[3] = {0, n64, n_all};
+      // Split the bra primitive pairs so one lane does at most ~lane_prims
+      // primitive quartets per task (the tensor keeps whole quartets).
+      const int nbp = c->pairs[gi].npp, nkp = K.ka * K.kb;
+      int chunk = nbp;
+      if (!full) chunk = std::max(1, std::min(nbp, c->tune[qc].lane_prims / std::max(1, nkp)));
+      // Register kernels: up to 32 kets per warp task (one per lane); the
+      // other engines: one ket per task, so every quartet gets its own warp.
+      const int per_task =
+          grad ? (c->grad_engine[qc] == kEngineReg ? 32 : 1) : (class_engine(c->tune[qc], qc) == kEngineReg ? 32 : 1);
+      for (int prec = 0; prec < 2; ++prec) {
+        for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
+          for (int b0 = 0; b0 < nbp; b0 += chunk) {
+            Task t;
+            t.bra = gi;
+            t.ket0 = K.start + k0;
+            t.nket = std::min(per_task, seg[prec + 1] - k0);
+            t.flags = b0 | (std::min(nbp, b0 + chunk) << 16);
+            out.lists[prec][qc].push_back(t);
+          }
+        }
+        out.nq[prec] += seg[prec + 1] - seg[prec];
+        out.cq[prec][qc] += seg[prec + 1] - seg[prec];
+        out.cp[prec][qc] += (long long)(seg[prec + 1] - seg[prec]) * nbp * nkp;
+      }
+      out.npq += (long long)n_all * c->pairs[gi].npp * K.ka * K.kb;
+    }
+  }
+}
+
+static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s,
+                       bool grad = false) {
   // Quartets pair a bra and a ket of the same molecule: ket blocks by molecule.
   std::vector<std::vector<int>> mol_blocks(c->n_mol);
   for (size_t cb = 0; cb < c->blocks.size(); ++cb) mol_blocks[c->blocks[cb].mol].push_back((int)cb);
-  for (size_t cb = 0; cb < c->blocks.size(); ++cb) {
-    const Block& B = c->blocks[cb];
-    for (int pi = 0; pi < B.count; ++pi) {
-      const int gi = B.start + pi;
-      const double Qi = c->pairs[gi].Q;
-      for (const int ckb : mol_blocks[B.mol]) {
-        const size_t ck = (size_t)ckb;
-        if (ck > cb) break;
-        const Block& K = c->blocks[ck];
-        const int limit = (ck == cb) ? pi + 1 : K.count;
-        const int n_all = prefix_count(c->pairs, K.start, limit, Qi, tau);
-        int n64 = n_all;
-        if (mode == JQC_PREC_FP32) n64 = 0;
-        if (mode == JQC_PREC_MIXED) n64 = std::min(n_all, prefix_count(c->pairs, K.start, limit, Qi, mixed_tau));
-        const int qc = quartet_class(B.pc, K.pc);
-        const int seg[3] = {0, n64, n_all};
-        // Split the bra primitive pairs so one lane does at most ~lane_prims
-        // primitive quartets per task (the tensor keeps whole quartets).
-        const int nbp = c->pairs[gi].npp, nkp = K.ka * K.kb;
-        int chunk = nbp;
-        if (!full) chunk = std::max(1, std::min(nbp, c->tune[qc].lane_prims / std::max(1, nkp)));
-        // Register classes: 32 kets per warp task (one per lane).  Warp-engine
-        // classes: one ket per task, so every quartet gets its own warp.
-        const int per_task =
-            grad ? (c->grad_engine[qc] == kEngineReg ? 32 : 1) : (class_engine(c->tune[qc], qc) == kEngineReg ? 32 : 1);
-        for (int prec = 0; prec < 2; ++prec) {
-          for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
-            for (int b0 = 0; b0 < nbp; b0 += chunk) {
-              Task t;
-              t.bra = gi;
-              t.ket0 = K.start + k0;
-              t.nket = std::min(per_task, seg[prec + 1] - k0);
-              t.flags = b0 | (std::min(nbp, b0 + chunk) << 16);
-              lists[prec][qc].push_back(t);
-            }
-          }
-          nq[prec] += seg[prec + 1] - seg[prec];
-          cq[prec][qc] += seg[prec + 1] - seg[prec];
-          cp[prec][qc] += (long long)(seg[prec + 1] - seg[prec]) * nbp * nkp;
-        }
-        npq += (long long)n_all * c->pairs[gi].npp * K.ka * K.kb;
+  const int n_pairs = (int)c->pairs.size();
+  std::vector<int> block_of(n_pairs);
+  for (size_t cb = 0; cb < c->blocks.size(); ++cb)
+    for (int k = 0; k < c->blocks[cb].count; ++k) block_of[c->blocks[cb].start + k] = (int)cb;
+  // Bra pairs split over host threads; the parts are concatenated in order,
+  // so the work list does not depend on the thread count.
+  int nthreads = (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (n_pairs < 4096) nthreads = 1;
+  std::vector<TaskPart> parts(nthreads);
+  {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthreads; ++t) {
+      const int g0 = (int)((long long)n_pairs * t / nthreads), g1 = (int)((long long)n_pairs * (t + 1) / nthreads);
+      if (nthreads == 1)
+        build_task_part(c, parts[t], g0, g1, block_of, mol_blocks, mode, mixed_tau, full, grad);
+      else
+        pool.emplace_back(build_task_part, c, std::ref(parts[t]), g0, g1, std::cref(block_of), std::cref(mol_blocks),
+                          mode, mixed_tau, full, grad);
+    }
+    for (auto& th : pool) th.join();
+  }
+  std::vector<Task> lists[2][kNumQuartetClasses];
+  long long nq[2] = {0, 0}, npq = 0;
+  long long cq[2][kNumQuartetClasses] = {}, cp[2][kNumQuartetClasses] = {};
+  for (int prec = 0; prec < 2; ++prec)
+    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+      size_t total = 0;
+      for (const TaskPart& p : parts) total += p.lists[prec][qc].size();
+      lists[prec][qc].reserve(total);
+      for (TaskPart& p : parts) {
+        lists[prec][qc].insert(lists[prec][qc].end(), p.lists[prec][qc].begin(), p.lists[prec][qc].end());
+        cq[prec][qc] += p.cq[prec][qc];
+        cp[prec][qc] += p.cp[prec][qc];
       }
     }
+  for (const TaskPart& p : parts) {
+    nq[0] += p.nq[0];
+    nq[1] += p.nq[1];
+    npq += p.npq;
   }
   // Longest tasks first inside each class launch (cost = lane primitive
   // quartets = bra primitive chunk x ket primitive pairs): a stable counting
