@@ -384,6 +384,28 @@ class _BatchFock:
         return sum(a.elapsed_time(c) for a, c in self.events) * 1e-3
 
 
+_HOST_EIGH_MAX_N = 512
+
+
+def _diag_all(groups, Fs):
+    """(eps, C) of X^T F X for every group.  The eigensolver runs on the host
+    cores for matrices up to a few hundred rows: a device eigh of that size
+    is latency bound (~3 ms a call) and would dominate the lock-step
+    iteration (measured: 2.6 s against 1.8 s over a 64-molecule SCF; threads
+    over the groups were slower still, the host solver is multithreaded
+    itself).  The products around it stay on the device."""
+    As = [g.X.transpose(1, 2) @ F @ g.X for g, F in zip(groups, Fs)]
+    out = []
+    for g, A in zip(groups, As):
+        if A.shape[-1] <= _HOST_EIGH_MAX_N:
+            e, V = torch.linalg.eigh(A.cpu())
+            e, V = e.to(A.device), V.to(A.device)
+        else:
+            e, V = torch.linalg.eigh(A)
+        out.append((e, g.X @ V))
+    return out
+
+
 class _Group:
     """Molecules of one (basis size, occupied count): their SCF state as
     stacked (G, n, n) tensors, so every step of the iteration is one batched
@@ -398,8 +420,8 @@ class _Group:
         self.Fh, self.Eh = [], []  # DIIS history, oldest first
 
     def diag(self, F):
-        e, V = torch.linalg.eigh(self.X.transpose(1, 2) @ F @ self.X)
-        return e, self.X @ V
+        """Orbital energies and coefficients of X^T F X (one group)."""
+        return _diag_all([self], [F])[0]
 
     def density(self, C):
         Co = C[:, :, :self.n_occ]
@@ -474,8 +496,7 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
         return g.H + J - 0.5 * K
 
     # core guess (rhf.py:111-121)
-    for g in groups:
-        _, C = g.diag(g.H)
+    for g, (_, C) in zip(groups, _diag_all(groups, [g.H for g in groups])):
         g.D = g.density(C)
     dens = {m: g.D[i] for g in groups for i, m in enumerate(g.members)}
     torch.cuda.synchronize()
@@ -487,7 +508,9 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     jk = fb.build(dens)
     for g in groups:
         g.F = fock(g, jk, g.D)
-        g.eps, g.C = g.diag(g.F)
+    for g, (eps, C) in zip(groups, _diag_all(groups, [g.F for g in groups])):
+        g.eps, g.C = eps, C
+    for g in groups:
         g.E = 0.5 * torch.sum(g.D * (g.H + g.F), dim=(1, 2))
         g.active = torch.ones(len(g.members), dtype=torch.bool, device=g.D.device)
         g.iters = torch.zeros(len(g.members), dtype=torch.int64, device=g.D.device)
@@ -501,14 +524,17 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
         dens = {m: g.D[i] for g in groups for i, m in enumerate(g.members) if not converged[m]}
         jk = fb.build(dens)
         Es, emaxs = [], []
+        errs, Fxs = [], []
         for g in groups:
-            act = g.active
             Fn = fock(g, jk, g.D)
             if config.damping > 0.0:
                 Fn = (1.0 - config.damping) * Fn + config.damping * g.F
             err = g.X.transpose(1, 2) @ (Fn @ g.D @ g.S - g.S @ g.D @ Fn) @ g.X  # diis.py:53-59
-            Fx = g.diis(Fn, err, config.diis_space)
-            eps, C = g.diag(Fx)
+            errs.append(err)
+            Fxs.append(g.diis(Fn, err, config.diis_space))
+        eigs = _diag_all(groups, Fxs)
+        for g, err, Fx, (eps, C) in zip(groups, errs, Fxs, eigs):
+            act = g.active
             D = g.density(C)
             E = 0.5 * torch.sum(D * (g.H + Fx), dim=(1, 2))
             a3 = act[:, None, None]
