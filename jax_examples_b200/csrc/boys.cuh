@@ -41,6 +41,11 @@ __device__ __forceinline__ int boys_round(float x) { return __float2int_rn(x); }
 // (FP32) aligned row at tabA[(M * kBoysRows + i) * 8], fetched with 16-byte
 // vector loads.
 constexpr int kBoysARow = 8;
+// After the (kBoysMaxM+1) x kBoysRows rows of the aligned table come the
+// kBoysRows values e^{-T_i}: below kBoysTMax, e^{-t} = e^{-T_i} e^{T_i - t}
+// with |T_i - t| <= 1/32, so a short Taylor series replaces the exponential.
+constexpr int kBoysExpOff = (kBoysMaxM + 1) * kBoysRows * kBoysARow;
+constexpr int kBoysAlignedSize = kBoysExpOff + kBoysRows;
 
 __device__ __forceinline__ void boys_row(const double* __restrict__ r, double (&v)[8]) {
   const double2* q = reinterpret_cast<const double2*>(r);
@@ -67,7 +72,12 @@ __device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F
     for (int k = KT - 2; k >= 0; --k) acc = v[k] + acc * (d * T(1.0 / (k + 1)));
     F[M] = acc;
     if (M > 0) {
-      const T e = boys_exp(-t);
+      // e^{-t} = e^{-T_i} e^{d}; the series of e^{d} to KT terms is as
+      // accurate as the Taylor series of F above (|d| <= 1/32)
+      T ed = T(1);
+#pragma unroll
+      for (int k = KT - 1; k >= 1; --k) ed = T(1) + ed * (d * T(1.0 / k));
+      const T e = __ldg(tabA + kBoysExpOff + i) * ed;
       const T t2 = t + t;
 #pragma unroll
       for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * T(1.0 / (2 * m + 1));

@@ -126,12 +126,12 @@ int boys_tables_all(int device, BoysTables* out) {
     std::vector<double> h(kBoysRows * kBoysCols);
     boys_fill_table(h.data());
     std::vector<float> hf(h.begin(), h.end());
-    const size_t na = (size_t)(kBoysMaxM + 1) * kBoysRows * kBoysARow;
-    std::vector<double> ha(na);
+    std::vector<double> ha(kBoysAlignedSize);
     for (int M = 0; M <= kBoysMaxM; ++M)
       for (int i = 0; i < kBoysRows; ++i)
         for (int k = 0; k < kBoysARow; ++k)
           ha[((size_t)M * kBoysRows + i) * kBoysARow + k] = h[(size_t)i * kBoysCols + M + k];
+    for (int i = 0; i < kBoysRows; ++i) ha[kBoysExpOff + i] = (double)expl(-(long double)i / kBoysGridInv);
     std::vector<float> haf(ha.begin(), ha.end());
     int prev = 0;
     JQC_CUDA_CHECK(cudaGetDevice(&prev));
