@@ -47,8 +47,9 @@ from .integrals import nuclear_repulsion_energy
 BATCH_DENS_TAU = 1e-30
 
 # Density screening of the gradient on the mixed path: the skipped quartets
-# change a (H2O)16 gradient by ~1e-6 Eh/bohr, inside the 1e-5 tolerance.
-MIXED_GRAD_TAU = 1e-10
+# change a (H2O)16 gradient by ~3.5e-6 Eh/bohr (1e-10: 1e-6, 1e-9: 1e-5),
+# inside the 1e-5 tolerance, for 38 ms instead of 75 ms unscreened.
+MIXED_GRAD_TAU = 3e-10
 
 
 class _Nuclei:
@@ -259,8 +260,8 @@ class _BatchFock:
       density screening at ``mixed_dens_tau``, a full rebuild every
       ``rebuild_every`` builds.  Once the largest DIIS error of the active
       molecules is below ``fp64_switch`` it switches to a full FP64 build and
-      incremental FP64 builds at the tight threshold 1e-12; convergence is
-      accepted only after ``fp64_tail_iters`` FP64 builds.
+      incremental FP64 builds screened at ``fp64_tail_dens_tau``; convergence
+      is accepted only after ``fp64_tail_iters`` FP64 builds.
     """
 
     def __init__(self, eng: BatchedERI, batch: MoleculeBatch, config: CalcConfig, use_graph: bool,
@@ -271,6 +272,7 @@ class _BatchFock:
         self.mixed = config.precision == "mixed"
         self.incremental = bool(config.incremental) and self.mixed
         self.mixed_tau = float(config.mixed_tau)
+        self.tail_tau = max(float(config.fp64_tail_dens_tau), BATCH_DENS_TAU)
         self.phase = "mixed" if self.mixed else "fp64"
         self.rebuild_every = rebuild_every
         self.fp64_builds = 0
@@ -286,7 +288,7 @@ class _BatchFock:
     def _settings(self, incremental: bool):
         if self.phase == "mixed":
             return "mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU) if incremental else BATCH_DENS_TAU
-        return "fp64", 1e-12 if incremental else BATCH_DENS_TAU
+        return "fp64", self.tail_tau if incremental else BATCH_DENS_TAU
 
     def _launch(self, incremental: bool):
         prec, tau = self._settings(incremental)
@@ -322,7 +324,7 @@ class _BatchFock:
             if self.mixed:
                 kinds += [("fp64", BATCH_DENS_TAU)]
             if self.incremental:
-                kinds += [("mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU)), ("fp64", 1e-12)]
+                kinds += [("mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU)), ("fp64", self.tail_tau)]
             t0 = time.perf_counter()
             for p_, t_ in kinds:
                 self.graphs[(p_, t_)] = self.eng.capture_jk(self.D, self.J, self.K, p_, self.mixed_tau, t_)

@@ -136,7 +136,10 @@ class CalcConfig(_Replace):
                     builds; at least this many FP64 iterations are run.
     incremental:    build F from the density change dD when true.
     mixed_dens_tau: density-screening threshold of the incremental builds
-                    in the mixed phase (the FP64 tail uses 1e-12).
+                    in the mixed phase.
+    fp64_tail_dens_tau: density-screening threshold of the incremental FP64
+                    builds after the switch (mixed mode only; plain FP64
+                    incremental builds screen at 1e-12).
     """
 
     method: str = "rhf"
@@ -156,6 +159,7 @@ class CalcConfig(_Replace):
     fp64_switch: float = 1e-5
     incremental: bool = True
     mixed_dens_tau: float = 1e-8
+    fp64_tail_dens_tau: float = 1e-10
 
 
 def make_molecule(elements, coords, atomic_numbers, charge: int = 0, spin: int = 0) -> Molecule:

@@ -172,6 +172,12 @@ struct TaskSet {
   DevBuf<Task> d;
   int off[2][kNumQuartetClasses] = {};
   int cnt[2][kNumQuartetClasses] = {};
+  // packed warp groups of the ket-outer register classes (JKParams::groups):
+  // gcnt groups, gcnt + 1 boundaries from goff, relative to the list's start
+  std::vector<int> gh;
+  DevBuf<int> gd;
+  int goff[2][kNumQuartetClasses] = {};
+  int gcnt[2][kNumQuartetClasses] = {};
   long long n_quartets[2] = {0, 0};
   long long n_prim_quartets = 0;
   long long class_quartets[2][kNumQuartetClasses] = {};
@@ -371,6 +377,54 @@ static void build_task_part(const jqc_ctx* c, TaskPart& out, int g0, int g1, con
   }
 }
 
+// Angular momentum sum of the bra pair of quartet class qc.
+static int qc_bra_lsum(int qc) { return pc_la(qc_bra(qc)) + pc_lb(qc_bra(qc)); }
+
+// Packs the tasks h[base, base + n) (one class list, sorted by descending
+// lane cost) into warp groups of at most 32 kets: inside each run of equal
+// cost, full tasks stay alone and the partial ones are paired largest with
+// smallest; the tasks of a group are made contiguous.  Appends the group
+// boundaries (relative to base, n_groups + 1 of them) to g and returns the
+// number of groups.
+template <typename Cost>
+static int pack_groups(std::vector<Task>& h, size_t base, size_t n, std::vector<int>& g, Cost lane_cost) {
+  std::vector<Task> part, out;
+  out.reserve(n);
+  int groups = 0;
+  g.push_back(0);
+  size_t i0 = 0;
+  while (i0 < n) {
+    size_t i1 = i0;
+    while (i1 < n && lane_cost(h[base + i1]) == lane_cost(h[base + i0])) ++i1;
+    part.clear();
+    for (size_t k = i0; k < i1; ++k) {
+      const Task& t = h[base + k];
+      if (t.nket >= 32) {
+        out.push_back(t);
+        g.push_back((int)out.size());
+        ++groups;
+      } else {
+        part.push_back(t);
+      }
+    }
+    std::stable_sort(part.begin(), part.end(), [](const Task& a, const Task& b) { return a.nket > b.nket; });
+    size_t lo = 0, hi = part.size();
+    while (lo < hi) {
+      int fill = part[lo].nket;
+      out.push_back(part[lo++]);
+      while (lo < hi && fill + part[hi - 1].nket <= 32) {
+        fill += part[hi - 1].nket;
+        out.push_back(part[--hi]);
+      }
+      g.push_back((int)out.size());
+      ++groups;
+    }
+    i0 = i1;
+  }
+  std::copy(out.begin(), out.end(), h.begin() + (long)base);
+  return groups;
+}
+
 static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool full, cudaStream_t s,
                        bool grad = false) {
   // Quartets pair a bra and a ket of the same molecule: ket blocks by molecule.
@@ -420,6 +474,7 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
   // quartets = bra primitive chunk x ket primitive pairs): a stable counting
   // sort on the cost, linear in the number of tasks.
   ts.h.clear();
+  ts.gh.clear();
   std::vector<int> cost, count;
   for (int prec = 0; prec < 2; ++prec)
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
@@ -438,8 +493,15 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
       const size_t base = ts.h.size();
       ts.h.resize(base + v.size());
       for (size_t k = 0; k < v.size(); ++k) ts.h[base + count[cmax - cost[k]]++] = v[k];
+      ts.goff[prec][qc] = (int)ts.gh.size();
+      ts.gcnt[prec][qc] = 0;
+      if (!full && !grad && qc_bra_lsum(qc) <= kKetOuterMaxLab && class_engine(c->tune[qc], qc) == kEngineReg)
+        ts.gcnt[prec][qc] = pack_groups(ts.h, base, v.size(), ts.gh, [c](const Task& t) {
+          return ((t.flags >> 16) - (t.flags & 0xffff)) * c->pairs[t.ket0].npp;
+        });
     }
   JQC_CUDA_CHECK(ts.d.upload(ts.h, s));
+  JQC_CUDA_CHECK(ts.gd.upload(ts.gh, s));
   ts.n_quartets[0] = nq[0];
   ts.n_quartets[1] = nq[1];
   ts.n_prim_quartets = npq;
@@ -565,6 +627,10 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
       p.threads = c->tune[qc].threads;
       p.persistent = c->tune[qc].persistent;
       p.engine = class_engine(c->tune[qc], qc);
+      if (ts->gcnt[prec][qc] > 0 && p.engine == kEngineReg) {
+        p.groups = ts->gd.ptr + ts->goff[prec][qc];
+        p.n_groups = ts->gcnt[prec][qc];
+      }
       if (class_ms) {
         JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));
         JQC_CUDA_CHECK(launch_jk(qc, prec == 1, p, s));

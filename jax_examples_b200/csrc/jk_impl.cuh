@@ -14,8 +14,13 @@
 //   K[a][d] += s v D[c][b], K[b][d] += s v D[c][a],
 //   K[a][c] += s v D[d][b], K[b][c] += s v D[d][a]
 // into accumulators A (J) and B (K); afterwards J = A + A^T, K = B + B^T.
-// J[a][b] is summed over the warp with shuffles before one atomic per
-// element; everything else goes to FP64 atomics directly.
+// J[a][b] is summed over the lanes of its bra pair with shuffles before one
+// atomic per element; everything else goes to FP64 atomics directly.
+//
+// Packed warps: in the classes whose bra angular sum is at most 2 (the
+// ket-outer loop order, every lane reads its own bra primitives) a warp takes
+// a group of tasks with at most 32 kets in all, so short ket runs of several
+// bra pairs fill one warp instead of leaving lanes idle.
 #pragma once
 
 #include "kernels.cuh"
@@ -48,10 +53,39 @@ struct JKBody {
     constexpr int NA = Cfg::NA, NB = Cfg::NB, ND = Cfg::ND;
     constexpr int NCDP = Cfg::NCDP;
 
-    const Task task = prm.tasks[warp];
+    // Ket-outer classes read their bra per lane, so one warp may hold the
+    // kets of several tasks (a packed group, lanes in task order): lane l
+    // belongs to the task whose run of kets covers l.  seg = that task's
+    // index in the group (-1 past the last ket).
+    constexpr bool kPacked = LA + LB <= kKetOuterMaxLab;
+    Task task;
+    bool in_range;
+    int kidx, seg = 0;
+    if constexpr (kPacked) {
+      const int g0 = prm.groups ? prm.groups[warp] : warp;
+      const int nt = prm.groups ? prm.groups[warp + 1] - g0 : 1;
+      const int cnt = lane < nt ? prm.tasks[g0 + lane].nket : 0;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int start = incl - cnt;
+      const unsigned starts = __reduce_or_sync(0xffffffffu, (cnt > 0 && start < 32) ? (1u << start) : 0u);
+      in_range = lane < total;
+      const unsigned upto = starts & (0xffffffffu >> (31 - lane));
+      const int ti = (in_range && upto != 0u) ? __popc(upto) - 1 : 0;
+      task = prm.tasks[g0 + ti];
+      kidx = task.ket0 + (in_range && upto != 0u ? lane - (31 - __clz(upto)) : 0);
+      seg = in_range ? ti : -1;
+    } else {
+      task = prm.tasks[warp];
+      in_range = lane < task.nket;
+      kidx = task.ket0 + (in_range ? lane : 0);
+    }
     const ShellPair bp = prm.pairs[task.bra];
-    const bool in_range = lane < task.nket;
-    const int kidx = task.ket0 + (in_range ? lane : 0);
     const ShellPair kp = prm.pairs[kidx];
     bool active = in_range;
     if (prm.dmax != nullptr && active) {
@@ -82,6 +116,21 @@ struct JKBody {
     if (kp.diag) s *= 0.5;
     if (task.bra == kidx) s *= 0.5;
 
+    // Segmented suffix sums over lanes of one task (packed warps): bit k of
+    // vmask says lane + 2^k holds the same task; the first lane of each task
+    // ends with its task's total.
+    unsigned vmask = 0u;
+    bool head = lane == 0;
+    if constexpr (kPacked) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const int so = __shfl_down_sync(0xffffffffu, seg, 1 << k);
+        if (lane + (1 << k) < 32 && so == seg) vmask |= 1u << k;
+      }
+      const int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+      head = seg >= 0 && (lane == 0 || sp != seg);
+    }
+
     const int n = prm.n;
     const int a0 = prm.ao[bp.a], b0 = prm.ao[bp.b], c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];
     for (int dd = 0; dd < prm.n_dens; ++dd) {
@@ -102,8 +151,17 @@ struct JKBody {
           constexpr int cdi = decltype(cdi_)::value;
           acc += double(out[ab][cdi]) * dcd[cdi];
         });
-        acc = warp_sum(2.0 * s * acc);
-        if (lane == 0) atomicAdd(Jm + (size_t)(a0 + ab / NB) * n + b0 + ab % NB, acc);
+        acc *= 2.0 * s;
+        if constexpr (kPacked) {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) {
+            const double t = __shfl_down_sync(0xffffffffu, acc, 1 << k);
+            if ((vmask >> k) & 1u) acc += t;
+          }
+        } else {
+          acc = warp_sum(acc);
+        }
+        if (head) atomicAdd(Jm + (size_t)(a0 + ab / NB) * n + b0 + ab % NB, acc);
       });
       if (!active) continue;
       // J[c][d]
@@ -165,7 +223,8 @@ __global__ void __launch_bounds__(kMaxJKThreads) jk_kernel(const JKParams prm) {
   constexpr int NS = class_split(LA, LB, LC, LD);
   __shared__ T sE[kMaxJKThreads / 32][3][LA + 1][LB + 1][LA + LB + 1];
   const int stride = int((gridDim.x * blockDim.x) >> 5);
-  for (int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); warp < prm.n_tasks; warp += stride) {
+  const int n_work = prm.groups ? prm.n_groups : prm.n_tasks;
+  for (int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); warp < n_work; warp += stride) {
     JKBody<T, LA, LB, LC, LD, NS> body{prm, warp, int(threadIdx.x & 31), sE[threadIdx.x >> 5]};
     dispatch_part<NS>(blockIdx.y, body);
     __syncwarp();  // every lane is done with the warp's bra E before the next task writes it
@@ -176,9 +235,11 @@ template <typename T, int LA, int LB, int LC, int LD>
 cudaError_t launch_jk_class(const JKParams& p, cudaStream_t s) {
   constexpr int NS = class_split(LA, LB, LC, LD);
   if (p.n_tasks == 0) return cudaSuccess;
+  // packed groups only where the kernel reads its bra per lane
+  if (p.groups != nullptr && LA + LB > kKetOuterMaxLab) return cudaErrorInvalidValue;
   const int threads = (p.threads == 64 || p.threads == 256) ? p.threads : 128;
   const int wpb = threads / 32;
-  long long blocks = (p.n_tasks + wpb - 1) / wpb;
+  long long blocks = ((p.groups ? p.n_groups : p.n_tasks) + wpb - 1) / wpb;
   if (p.persistent) {
     // resident blocks per SM for this block size, times the SM count
     static int occ[3] = {0, 0, 0};

@@ -38,6 +38,11 @@ struct JKParams {
   int threads = 128;       // threads per block (64, 128, 256)
   int persistent = 0;      // 1: grid capped at the resident blocks, warps stride over tasks
   int engine = kEngineReg; // JKEngine
+  // Packed warps (register kernels of bra angular sum <= 2): warp w takes
+  // tasks groups[w] .. groups[w+1]-1, at most 32 kets in all, lane by lane.
+  // nullptr: one task per warp.
+  const int* groups = nullptr;
+  int n_groups = 0;
 };
 
 constexpr int kMaxJKThreads = 256;

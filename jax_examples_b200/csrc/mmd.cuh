@@ -197,7 +197,8 @@ __device__ __forceinline__ void prim_quartet_R(const PPT& bp, const PPT& kp, con
 }
 
 // Classes whose bra angular sum is at most this loop over ket primitives
-// outermost (see quartet_accumulate).
+// outermost (see quartet_accumulate) and read their bra per lane, so the
+// register J/K kernel can pack the kets of several bra pairs into one warp.
 constexpr int kKetOuterMaxLab = 2;
 
 // Accumulates the contracted block (ab|cd) for the ket Cartesian pairs of

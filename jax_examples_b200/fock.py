@@ -17,9 +17,12 @@ the precision policy of the mixed path:
   density; 3e-8 and a threshold that follows the DIIS error upward already
   cost more iterations than they save).  When the SCF error
   drops below ``fp64_switch`` the builder switches to FP64 with a full
-  rebuild and then tight-threshold incremental FP64 builds, and convergence
-  is only accepted after ``fp64_tail_iters`` of them: the final energy is an
-  FP64 energy.
+  rebuild (which drops the errors of the mixed phase) and then incremental
+  FP64 builds screened at ``fp64_tail_dens_tau`` (1e-10: (H2O)16 ends within
+  2e-7 Eh of the plain FP64 energy; the unscreened full rebuild at the switch
+  is what keeps it there, without it the mixed-phase errors stay at 1e-5 Eh),
+  and convergence is only accepted after ``fp64_tail_iters`` of them: the
+  final energy is an FP64 energy.
 """
 
 from __future__ import annotations
@@ -101,12 +104,14 @@ class FockBuilder:
         self.rebuild_every = rebuild_every
         self.dens_tau = dens_tau
         self.mixed_dens_tau = float(getattr(config, "mixed_dens_tau", 1e-8))
+        self.tail_dens_tau = float(getattr(config, "fp64_tail_dens_tau", dens_tau))
         self.phase = "mixed" if (self.precision == "mixed" and self.direct) else "fp64"
         self.fp64_builds_after_switch = 0
         self.switched = self.phase == "fp64"
         self._prev = None  # (D stack, J stack, K stack) of the last build
         self._since_full = 0
         self._events = []  # (start, end) CUDA events of every build
+        self._kinds = []  # "<precision>-full" / "<precision>-inc" of every build
         self.log = {"builds_mixed": 0, "builds_fp64": 0, "incremental_builds": 0, "jk_seconds": 0.0}
 
     # ----------------------------------------------------------------- core
@@ -128,15 +133,22 @@ class FockBuilder:
         use_inc = self.incremental and self._prev is not None and self._since_full < self.rebuild_every
         if use_inc and self._prev[0].shape == D.shape:
             dD = D - self._prev[0]
-            tau = max(self.mixed_dens_tau, self.dens_tau) if prec == "mixed" else self.dens_tau
+            if prec == "mixed":
+                tau = max(self.mixed_dens_tau, self.dens_tau)
+            elif self.precision == "mixed":
+                tau = max(self.tail_dens_tau, self.dens_tau)  # FP64 tail of the mixed policy
+            else:
+                tau = self.dens_tau
             dJ, dK = self.eri.jk(dD, precision=prec, mixed_tau=self.mixed_tau, dens_tau=tau)
             J = self._prev[1] + dJ
             K = self._prev[2] + dK
             self._since_full += 1
             self.log["incremental_builds"] += 1
+            self._kinds.append(prec + "-inc")
         else:
             J, K = self.eri.jk(D, precision=prec, mixed_tau=self.mixed_tau)
             self._since_full = 0
+            self._kinds.append(prec + "-full")
         if self.incremental:
             self._prev = (D, J, K)
         e1.record()
@@ -170,9 +182,12 @@ class FockBuilder:
         return self.phase == "fp64" and self.fp64_builds_after_switch >= self.fp64_tail
 
     def record(self) -> dict:
-        """Build counters and the device time of all J/K builds (CUDA events)."""
+        """Build counters, the device time of all J/K builds (CUDA events) and
+        each build's kind and milliseconds."""
         if self._events:
             self._events[-1][1].synchronize()
-            self.log["jk_seconds"] = sum(a.elapsed_time(b) for a, b in self._events) * 1e-3
+            ms = [a.elapsed_time(b) for a, b in self._events]
+            self.log["jk_seconds"] = sum(ms) * 1e-3
+            self.log["build_ms"] = [[k, round(t, 3)] for k, t in zip(self._kinds, ms)]
         return dict(self.log, precision=self.precision, mixed_tau=self.mixed_tau,
                     incremental=self.incremental)
