@@ -33,6 +33,8 @@ __device__ __forceinline__ double boys_exp(double x) { return exp(x); }
 __device__ __forceinline__ float boys_exp(float x) { return expf(x); }
 __device__ __forceinline__ double boys_sqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float boys_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double boys_rsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float boys_rsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ int boys_round(double x) { return __double2int_rn(x); }
 __device__ __forceinline__ int boys_round(float x) { return __float2int_rn(x); }
 
@@ -42,10 +44,12 @@ __device__ __forceinline__ int boys_round(float x) { return __float2int_rn(x); }
 // vector loads.
 constexpr int kBoysARow = 8;
 // After the (kBoysMaxM+1) x kBoysRows rows of the aligned table come the
-// kBoysRows values e^{-T_i}: below kBoysTMax, e^{-t} = e^{-T_i} e^{T_i - t}
-// with |T_i - t| <= 1/32, so a short Taylor series replaces the exponential.
+// kBoysExpRows values e^{-T_i} (T_i up to kBoysExpTEnd): e^{-t} = e^{-T_i}
+// e^{T_i - t} with |T_i - t| <= 1/32, so a short Taylor series replaces the
+// exponential on both sides of kBoysTMax, and the lanes of a warp that fall
+// on different sides of it share that part of the work.
 constexpr int kBoysExpOff = (kBoysMaxM + 1) * kBoysRows * kBoysARow;
-constexpr int kBoysAlignedSize = kBoysExpOff + kBoysRows;
+constexpr int kBoysAlignedSize = kBoysExpOff + kBoysExpRows;
 
 __device__ __forceinline__ void boys_row(const double* __restrict__ r, double (&v)[8]) {
   const double2* q = reinterpret_cast<const double2*>(r);
@@ -59,35 +63,41 @@ __device__ __forceinline__ void boys_row(const float* __restrict__ r, float (&v)
 }
 
 // Writes F_0 .. F_M at T into F[0..M] from the aligned table `tabA`.
+// e^{-t} comes from the tabulated e^{-T_i} for every t (0 beyond the end of
+// its grid), so only the few operations that differ between the Taylor
+// branch (t < kBoysTMax) and the asymptotic branch diverge inside a warp.
 template <typename T, int M>
 __device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F)[M + 1]) {
   constexpr int KT = BoysConst<T>::kTaylor;
+  const T tc = t < T(kBoysExpTEnd) ? t : T(kBoysExpTEnd);
+  const int i = boys_round(tc * T(kBoysGridInv));
+  const T d = T(i) * T(1.0 / kBoysGridInv) - tc;  // T_i - t, |d| <= 1/32
+  T e = T(0);
+  if constexpr (M > 0) {
+    // e^{-t} = e^{-T_i} e^{d}; the series of e^{d} to KT terms is as accurate
+    // as the Taylor series of F below
+    T ed = T(1);
+#pragma unroll
+    for (int k = KT - 1; k >= 1; --k) ed = T(1) + ed * (d * T(1.0 / k));
+    e = __ldg(tabA + kBoysExpOff + i) * ed;
+  }
   if (t < T(kBoysTMax)) {
-    const int i = boys_round(t * T(kBoysGridInv));
-    const T d = T(i) * T(1.0 / kBoysGridInv) - t;  // T_i - t
     T v[8];
     boys_row(tabA + (M * kBoysRows + i) * kBoysARow, v);
     T acc = v[KT - 1];
 #pragma unroll
     for (int k = KT - 2; k >= 0; --k) acc = v[k] + acc * (d * T(1.0 / (k + 1)));
     F[M] = acc;
-    if (M > 0) {
-      // e^{-t} = e^{-T_i} e^{d}; the series of e^{d} to KT terms is as
-      // accurate as the Taylor series of F above (|d| <= 1/32)
-      T ed = T(1);
-#pragma unroll
-      for (int k = KT - 1; k >= 1; --k) ed = T(1) + ed * (d * T(1.0 / k));
-      const T e = __ldg(tabA + kBoysExpOff + i) * ed;
+    if constexpr (M > 0) {
       const T t2 = t + t;
 #pragma unroll
       for (int m = M - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * T(1.0 / (2 * m + 1));
     }
   } else {
-    const T inv_t = T(1) / t;
-    F[0] = T(0.88622692545275801364908374167057) * boys_sqrt(inv_t);  // sqrt(pi)/2
-    if (M > 0) {
-      const T e = boys_exp(-t);
-      const T half_inv_t = T(0.5) * inv_t;
+    const T r = boys_rsqrt(t);
+    F[0] = T(0.88622692545275801364908374167057) * r;  // sqrt(pi)/2 / sqrt(t)
+    if constexpr (M > 0) {
+      const T half_inv_t = T(0.5) * (r * r);
 #pragma unroll
       for (int m = 0; m < M; ++m) F[m + 1] = (T(2 * m + 1) * F[m] - e) * half_inv_t;
     }

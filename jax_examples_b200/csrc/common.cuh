@@ -24,6 +24,10 @@ constexpr int kBoysRows = 36 * kBoysGridInv + 1;
 constexpr int kBoysTaylor = 8;            // Taylor terms (|dT| <= 1/32 -> ~2e-17 rel)
 constexpr int kBoysTaylorF = 5;           // FP32 Taylor terms
 constexpr int kBoysCols = kBoysMaxM + kBoysTaylor + 1;
+// The values e^{-T_i} for the Boys recursions continue the grid to T = 746,
+// where e^{-T} underflows to 0 in FP64 (and long before in FP32).
+constexpr int kBoysExpTEnd = 746;
+constexpr int kBoysExpRows = kBoysExpTEnd * kBoysGridInv + 1;
 
 void set_error(const std::string& msg);
 
