@@ -465,11 +465,12 @@ def run_ours(args):
         # both paths' work lists are built, and the kernels of both paths
         # loaded, before the timed SCF runs
         t_wl = time.perf_counter()
-        eng.stats("mixed", 1e-7)
+        chosen_tau = CalcConfig().mixed_tau
+        eng.stats("mixed", chosen_tau)
         torch.cuda.synchronize()
         t_wl = time.perf_counter() - t_wl
         for prec, tau in (("mixed", 0.0), ("mixed", 1e-8), ("fp64", 1e-10)):
-            eng.jk(D, precision=prec, mixed_tau=1e-7, dens_tau=tau)
+            eng.jk(D, precision=prec, mixed_tau=chosen_tau, dens_tau=tau)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         # plain: a full FP64 build every iteration (the reference's Fock build)

@@ -130,7 +130,10 @@ class CalcConfig(_Replace):
     precision:      "fp64" (plain kernel) or "mixed" (FP32 for quartets whose
                     Schwarz bound is below ``mixed_tau``).
     schwarz_tau:    quartets with Q_ij*Q_kl*max|D| below this are skipped.
-    mixed_tau:      FP32/FP64 split on the quartet Schwarz bound.
+    mixed_tau:      FP32/FP64 split on the quartet Schwarz bound (1e-4: on
+                    (H2O)16 the mixed builds are ~7% faster than at 1e-7 with
+                    the same iterations and final error; 1e-2 and above cost
+                    extra SCF iterations).
     fp64_tail_iters: in mixed mode, once the SCF is within ``fp64_switch`` of
                     convergence the remaining iterations use incremental FP64
                     builds; at least this many FP64 iterations are run.
@@ -154,7 +157,7 @@ class CalcConfig(_Replace):
     profile: bool = False
     precision: str = "fp64"
     schwarz_tau: float = 1e-13
-    mixed_tau: float = 1e-7
+    mixed_tau: float = 1e-4
     fp64_tail_iters: int = 2
     fp64_switch: float = 1e-5
     incremental: bool = True

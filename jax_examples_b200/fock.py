@@ -97,7 +97,7 @@ class FockBuilder:
             if not torch.is_tensor(ERI):
                 self.eri = torch.as_tensor(np.asarray(ERI), dtype=torch.float64)
         self.precision = getattr(config, "precision", "fp64")
-        self.mixed_tau = float(getattr(config, "mixed_tau", 1e-7))
+        self.mixed_tau = float(getattr(config, "mixed_tau", 1e-4))
         self.incremental = bool(getattr(config, "incremental", False)) and self.direct
         self.fp64_tail = int(getattr(config, "fp64_tail_iters", 2))
         self.fp64_switch = float(getattr(config, "fp64_switch", 1e-5))
