@@ -50,39 +50,6 @@ struct ColSmem {
 
 constexpr int kColWarps = 4;
 
-// In-place R^n_tuv recursion (the order of hermite_R in mmd.cuh), lanes
-// parallel over the entries of one total order.
-template <typename T, int L>
-__device__ __forceinline__ void col_hermite_R(T* R, const T* Rn, T X, T Y, T Z, int lane) {
-  if (lane == 0) R[0] = Rn[L];
-  __syncwarp();
-#pragma unroll 1
-  for (int n = L - 1; n >= 0; --n) {
-#pragma unroll 1
-    for (int s = L - n; s >= 1; --s) {
-      const int base = nherm(s - 1);
-      for (int k = lane; k < ncart(s); k += 32) {
-        const int t = cart_lx(s, k), u = cart_ly(s, k), v = s - t - u;
-        T val;
-        if (t > 0) {
-          val = X * R[herm_index(t - 1, u, v)];
-          if (t > 1) val += T(t - 1) * R[herm_index(t - 2, u, v)];
-        } else if (u > 0) {
-          val = Y * R[herm_index(t, u - 1, v)];
-          if (u > 1) val += T(u - 1) * R[herm_index(t, u - 2, v)];
-        } else {
-          val = Z * R[herm_index(t, u, v - 1)];
-          if (v > 1) val += T(v - 1) * R[herm_index(t, u, v - 2)];
-        }
-        R[base + k] = val;
-      }
-      __syncwarp();
-    }
-    if (lane == 0) R[0] = Rn[n];
-    __syncwarp();
-  }
-}
-
 // Bra E coefficients of one bra primitive pair (lanes 0..2, one axis each).
 // The caller synchronises the warp before (earlier readers) and after.
 template <typename T, int LA, int LB, int LC, int LD>
@@ -116,7 +83,7 @@ __device__ __forceinline__ void col_add_prim(ColSmem<T, LA, LB, LC, LD>* sm, con
     sm->Rn[lane] = pref * boys_single<T>(tb, lane, tab);
   }
   __syncwarp();
-  col_hermite_R<T, L>(sm->R, sm->Rn, X, Y, Z, lane);
+  warp_hermite_R<T, L>(sm->R, sm->Rn, X, Y, Z, lane);
   for (int c = lane; c < NCD; c += 32) {
     const int ci = c / ND, di = c - (c / ND) * ND;
     const int cx = cart_lx(LC, ci), cy = cart_ly(LC, ci), cz = LC - cx - cy;

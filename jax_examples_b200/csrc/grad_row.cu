@@ -7,7 +7,8 @@
 // primitive quartet, lanes 0..2 build the bra E up to (la+1, lb+1) with the
 // derivative coefficients DA = 2 alpha E_{i+1} - i E_{i-1}, DB likewise,
 // lanes 3..5 the signed ket E up to lc+1 with DC, lanes 0..L+1 the Boys
-// values, and R_tuv up to L+1 is built cooperatively in shared memory.  Each
+// values, and R_tuv up to L+1 is built cooperatively in shared memory
+// (warp_hermite_R).  Each
 // lane then, for its row ab:
 //   Fg[h'] = sum_cd Gamma_abcd F^cd_h'            (ket Hermite h' <= lc+ld)
 //   Z[h]   = sum_h' Fg[h'] R_{h+h'}                (h <= la+lb+1)
@@ -48,37 +49,6 @@ struct GRowSmem {
 };
 
 constexpr int kGRowWarps = 4;
-
-template <int L>
-__device__ __forceinline__ void gr_hermite_R(double* R, const double* Rn, double X, double Y, double Z, int lane) {
-  if (lane == 0) R[0] = Rn[L];
-  __syncwarp();
-#pragma unroll 1
-  for (int n = L - 1; n >= 0; --n) {
-#pragma unroll 1
-    for (int s = L - n; s >= 1; --s) {
-      const int base = nherm(s - 1);
-      for (int k = lane; k < ncart(s); k += 32) {
-        const int t = cart_lx(s, k), u = cart_ly(s, k), v = s - t - u;
-        double val;
-        if (t > 0) {
-          val = X * R[herm_index(t - 1, u, v)];
-          if (t > 1) val += (t - 1) * R[herm_index(t - 2, u, v)];
-        } else if (u > 0) {
-          val = Y * R[herm_index(t, u - 1, v)];
-          if (u > 1) val += (u - 1) * R[herm_index(t, u - 2, v)];
-        } else {
-          val = Z * R[herm_index(t, u, v - 1)];
-          if (v > 1) val += (v - 1) * R[herm_index(t, u, v - 2)];
-        }
-        R[base + k] = val;
-      }
-      __syncwarp();
-    }
-    if (lane == 0) R[0] = Rn[n];
-    __syncwarp();
-  }
-}
 
 struct F6 {
   double v[6];
@@ -143,22 +113,34 @@ __device__ __noinline__ F6 row_bra(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
       Z[h] += f * sm->R[herm_index(gr_ht(h) + gr_ht(k), gr_hu(h) + gr_hu(k), gr_hv(h) + gr_hv(k))];
     });
   });
-  // two partial sums per component (even / odd h) halve the dependency chains
-  double acc[2][6] = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
+  // The six derivative sums factor through one partial sum per axis:
+  // dA_x = sum_t DA^x_t S^x_t with S^x_t = sum_{u,v} E^y_u E^z_v Z_tuv, and
+  // likewise for y, z and the B centre.
+  double sx[LAB + 2], sy[LAB + 2], sz[LAB + 2];
+  static_for<LAB + 2>([&](auto t_) {
+    constexpr int t = decltype(t_)::value;
+    sx[t] = 0.0;
+    sy[t] = 0.0;
+    sz[t] = 0.0;
+  });
   static_for<NH1>([&](auto h_) {
     constexpr int h = decltype(h_)::value;
-    constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h), q = h & 1;
+    constexpr int t = gr_ht(h), u = gr_hu(h), v = gr_hv(h);
     const double z = Z[h];
-    acc[q][0] += dax[t] * ey[u] * ez[v] * z;
-    acc[q][1] += ex[t] * day[u] * ez[v] * z;
-    acc[q][2] += ex[t] * ey[u] * daz[v] * z;
-    acc[q][3] += dbx[t] * ey[u] * ez[v] * z;
-    acc[q][4] += ex[t] * dby[u] * ez[v] * z;
-    acc[q][5] += ex[t] * ey[u] * dbz[v] * z;
+    sx[t] += (ey[u] * ez[v]) * z;
+    sy[u] += (ex[t] * ez[v]) * z;
+    sz[v] += (ex[t] * ey[u]) * z;
   });
-  F6 out;
-#pragma unroll
-  for (int k = 0; k < 6; ++k) out.v[k] = acc[0][k] + acc[1][k];
+  F6 out = {{0, 0, 0, 0, 0, 0}};
+  static_for<LAB + 2>([&](auto t_) {
+    constexpr int t = decltype(t_)::value;
+    out.v[0] += dax[t] * sx[t];
+    out.v[1] += day[t] * sy[t];
+    out.v[2] += daz[t] * sz[t];
+    out.v[3] += dbx[t] * sx[t];
+    out.v[4] += dby[t] * sy[t];
+    out.v[5] += dbz[t] * sz[t];
+  });
   return out;
 }
 
@@ -203,26 +185,57 @@ __device__ __noinline__ F3 row_ket(const GRowSmem<LA, LB, LC, LD>* sm, int ab) {
     constexpr int cd = decltype(cd_)::value, ci = cd / ND, di = cd % ND;
     constexpr int cx = cart_lx(LC, ci), cy = cart_ly(LC, ci), cz = cart_lz(LC, ci);
     constexpr int dx = cart_lx(LD, di), dy = cart_ly(LD, di), dz = cart_lz(LD, di);
+    constexpr int TX = cx + dx, TY = cy + dy, TZ = cz + dz;
     const double w = Gr[cd];
-    double sx = 0.0, sy = 0.0, sz = 0.0;
-    static_for<cx + dx + 2>([&](auto t_) {
+    // dE/dC_x = sum_t DC^x_t sum_u F^y_u sum_v F^z_v W_tuv (y, z likewise),
+    // factored through P_tu = sum_v F^z_v W_tuv and Q_v = sum_{t,u} F^x_t F^y_u W_tuv
+    double P[TX + 2][TY + 2];
+    static_for<TX + 2>([&](auto t_) {
       constexpr int t = decltype(t_)::value;
-      static_for<cy + dy + 2>([&](auto u_) {
+      static_for<TY + 2>([&](auto u_) {
         constexpr int u = decltype(u_)::value;
-        static_for<cz + dz + 2>([&](auto v_) {
-          constexpr int v = decltype(v_)::value;
-          constexpr int over = (t > cx + dx) + (u > cy + dy) + (v > cz + dz);
-          if constexpr (over <= 1) {
-            const double wk = W[herm_index(t, u, v)];
-            if constexpr (u <= cy + dy && v <= cz + dz)
-              sx += sm->DC[0][cx][dx][t] * sm->Fk[1][cy][dy][u] * sm->Fk[2][cz][dz][v] * wk;
-            if constexpr (t <= cx + dx && v <= cz + dz)
-              sy += sm->Fk[0][cx][dx][t] * sm->DC[1][cy][dy][u] * sm->Fk[2][cz][dz][v] * wk;
-            if constexpr (t <= cx + dx && u <= cy + dy)
-              sz += sm->Fk[0][cx][dx][t] * sm->Fk[1][cy][dy][u] * sm->DC[2][cz][dz][v] * wk;
-          }
-        });
+        if constexpr (t <= TX || u <= TY) {
+          double acc = 0.0;
+          static_for<TZ + 1>([&](auto v_) {
+            constexpr int v = decltype(v_)::value;
+            acc += sm->Fk[2][cz][dz][v] * W[herm_index(t, u, v)];
+          });
+          P[t][u] = acc;
+        }
       });
+    });
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    static_for<TX + 2>([&](auto t_) {
+      constexpr int t = decltype(t_)::value;
+      double a = 0.0;
+      static_for<TY + 1>([&](auto u_) {
+        constexpr int u = decltype(u_)::value;
+        a += sm->Fk[1][cy][dy][u] * P[t][u];
+      });
+      sx += sm->DC[0][cx][dx][t] * a;
+    });
+    static_for<TY + 2>([&](auto u_) {
+      constexpr int u = decltype(u_)::value;
+      double a = 0.0;
+      static_for<TX + 1>([&](auto t_) {
+        constexpr int t = decltype(t_)::value;
+        a += sm->Fk[0][cx][dx][t] * P[t][u];
+      });
+      sy += sm->DC[1][cy][dy][u] * a;
+    });
+    static_for<TZ + 2>([&](auto v_) {
+      constexpr int v = decltype(v_)::value;
+      double q = 0.0;
+      static_for<TX + 1>([&](auto t_) {
+        constexpr int t = decltype(t_)::value;
+        double a = 0.0;
+        static_for<TY + 1>([&](auto u_) {
+          constexpr int u = decltype(u_)::value;
+          a += sm->Fk[1][cy][dy][u] * W[herm_index(t, u, v)];
+        });
+        q += sm->Fk[0][cx][dx][t] * a;
+      });
+      sz += sm->DC[2][cz][dz][v] * q;
     });
     out.v[0] += w * sx;
     out.v[1] += w * sy;
@@ -343,7 +356,7 @@ __global__ void __launch_bounds__(32 * kGRowWarps, grad_row_min_blocks(LA, LB, L
           sm->Rn[lane] = pref * boys_single<double>(tb, lane, prm.boys);
         }
         __syncwarp();
-        gr_hermite_R<L + 1>(sm->R, sm->Rn, X, Y, Z, lane);
+        warp_hermite_R<double, L + 1>(sm->R, sm->Rn, X, Y, Z, lane);
 #pragma unroll 1
         for (int ab = lane; ab < NAB; ab += 32) {
           const F6 fb = row_bra<LA, LB, LC, LD>(sm, ab);

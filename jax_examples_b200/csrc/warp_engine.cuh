@@ -17,6 +17,76 @@
 
 namespace jqc {
 
+// One step of the in-place Hermite recursion for each Hermite index h of
+// total order s >= 1 (t, u, v): R_h = PQ_axis R_src1 + coef R_src2 along the
+// first axis with a nonzero index (R_{t,u,v} = X R_{t-1,u,v} + (t-1)
+// R_{t-2,u,v}, ...), packed as src1 | src2 << 9 | coef << 18 | axis << 22
+// (src2 = coef = 0 where the second term is absent).  Built at compile time;
+// the warp recursions below read one code per lane and order instead of
+// decoding (t, u, v) with integer loops.
+constexpr int kRCodeMaxL = 10;
+struct RCodeTable {
+  int v[nherm(kRCodeMaxL)];
+  constexpr RCodeTable() : v() {
+    for (int s = 1; s <= kRCodeMaxL; ++s)
+      for (int k = 0; k < ncart(s); ++k) {
+        const int t = cart_lx(s, k), u = cart_ly(s, k), w = s - t - u;
+        int ax = 2, s1 = 0, s2 = 0, cf = 0;
+        if (t > 0) {
+          ax = 0;
+          s1 = herm_index(t - 1, u, w);
+          if (t > 1) s2 = herm_index(t - 2, u, w), cf = t - 1;
+        } else if (u > 0) {
+          ax = 1;
+          s1 = herm_index(t, u - 1, w);
+          if (u > 1) s2 = herm_index(t, u - 2, w), cf = u - 1;
+        } else {
+          s1 = herm_index(t, u, w - 1);
+          if (w > 1) s2 = herm_index(t, u, w - 2), cf = w - 1;
+        }
+        v[nherm(s - 1) + k] = s1 | (s2 << 9) | (cf << 18) | (ax << 22);
+      }
+  }
+};
+__device__ constexpr RCodeTable kRCode{};
+
+// R^0_tuv for all t+u+v <= L into R (warp-shared, Hermite layout) from
+// Rn[n] = R^n_000, in place: level n = L-1 .. 0, order s = L-n .. 1 (highest
+// first, so the lower orders still hold level n+1), lanes over the
+// components of one order.  Fully unrolled; each lane keeps its recursion
+// codes in registers.
+template <typename T, int L>
+__device__ __forceinline__ void warp_hermite_R(T* R, const T* Rn, T X, T Y, T Z, int lane) {
+  static_assert(L <= kRCodeMaxL, "recursion table too small");
+  int code[L + 1][2];
+  static_for<L>([&](auto i_) {
+    constexpr int s = decltype(i_)::value + 1;
+    code[s][0] = lane < ncart(s) ? __ldg(kRCode.v + nherm(s - 1) + lane) : 0;
+    code[s][1] = lane + 32 < ncart(s) ? __ldg(kRCode.v + nherm(s - 1) + lane + 32) : 0;
+  });
+  if (lane == 0) R[0] = Rn[L];
+  __syncwarp();
+  static_for<L>([&](auto i_) {
+    constexpr int n = L - 1 - decltype(i_)::value;
+    static_for<L - n>([&](auto j_) {
+      constexpr int s = L - n - decltype(j_)::value;
+      static_for<(ncart(s) + 31) / 32>([&](auto r_) {
+        constexpr int r = decltype(r_)::value;
+        const int k = 32 * r + lane;
+        if (k < ncart(s)) {
+          const int c = code[s][r];
+          const int ax = c >> 22;
+          const T pq = ax == 0 ? X : (ax == 1 ? Y : Z);
+          R[nherm(s - 1) + k] = pq * R[c & 511] + T((c >> 18) & 15) * R[(c >> 9) & 511];
+        }
+      });
+      __syncwarp();
+    });
+    if (lane == 0) R[0] = Rn[n];
+    __syncwarp();
+  });
+}
+
 constexpr int kWarpMaxL = 8;
 constexpr int kWarpMaxHerm = nherm(kWarpMaxL);          // 165
 constexpr int kWarpMaxHab = nherm(4);                    // 35 bra Hermite functions
