@@ -209,8 +209,11 @@ int jqc_set_tuning(jqc_ctx *ctx, const int *cfg84);
 
 /* Engine of the ERI-derivative adjoint for one quartet class: 0 register
  * kernels (L <= 4), 1 row engine (bra pair dp or dd; one warp per quartet,
- * lane = bra Cartesian pair), 2 runtime-class warp engine.  Defaults: row
- * engine for L >= 5, register kernels up to L = 4.  No reference
+ * lane = bra Cartesian pair), 2 runtime-class warp engine, 3 register
+ * kernels with the bra-centre and ket-centre forces in separate block parts
+ * (L <= 4; half the per-thread state, R and Boys computed twice).
+ * Defaults: row engine for L >= 5, engine 3 for (dp|ss) and (dp|ps),
+ * register kernels for the other classes up to L = 4.  No reference
  * counterpart. */
 int jqc_set_grad_engine(jqc_ctx *ctx, int quartet_class, int engine);
 int jqc_get_grad_engine(jqc_ctx *ctx, int *engines21);

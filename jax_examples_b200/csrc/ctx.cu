@@ -215,11 +215,17 @@ static int class_engine(const ClassTune& t, int qc) { return t.engine < 0 ? defa
 // kernels up to L = 4, the warp engine otherwise.
 static int default_grad_engine(int qc) {
   if (has_grad_row_class(qc) && qc_L(qc) >= 5) return kEngineCol;
+  // dp bras in the register kernels: the split sides halve the time
+  // ((dp|ss) 4.0 -> 2.2 ms, (dp|ps) 7.4 -> 3.7 ms on (H2O)16); for the other
+  // classes computing R twice costs more than the spills it removes
+  if (is_grad_reg_class(qc) && qc_bra(qc) == 4) return kGradEngineRegSplit;
   return is_grad_reg_class(qc) ? kEngineReg : kEngineWarp;
 }
+// The register gradient kernels (one or two sides): 32 kets per task.
+static bool grad_reg_engine(int e) { return e == kEngineReg || e == kGradEngineRegSplit; }
 static bool grad_engine_valid(int e, int qc) {
-  return (e == kEngineReg && is_grad_reg_class(qc)) || (e == kEngineCol && has_grad_row_class(qc)) ||
-         e == kEngineWarp;
+  return ((e == kEngineReg || e == kGradEngineRegSplit) && is_grad_reg_class(qc)) ||
+         (e == kEngineCol && has_grad_row_class(qc)) || e == kEngineWarp;
 }
 static bool engine_valid(int e, int qc) {
   return (e == kEngineReg && is_reg_class(qc)) || (e == kEngineCol && has_col_class(qc)) || e == kEngineWarp;
@@ -356,7 +362,7 @@ static void build_task_part(const jqc_ctx* c, TaskPart& out, int g0, int g1, con
       // Register kernels: up to 32 kets per warp task (one per lane); the
       // other engines: one ket per task, so every quartet gets its own warp.
       const int per_task =
-          grad ? (c->grad_engine[qc] == kEngineReg ? 32 : 1) : (class_engine(c->tune[qc], qc) == kEngineReg ? 32 : 1);
+          grad ? (grad_reg_engine(c->grad_engine[qc]) ? 32 : 1) : (class_engine(c->tune[qc], qc) == kEngineReg ? 32 : 1);
       for (int prec = 0; prec < 2; ++prec) {
         for (int k0 = seg[prec]; k0 < seg[prec + 1]; k0 += per_task) {
           for (int b0 = 0; b0 < nbp; b0 += chunk) {
@@ -1125,7 +1131,8 @@ int jqc_grad2e_ex(jqc_ctx* c, int n_dens, const double* D, double j_scale, doubl
     const int pb = qc_bra(qc), pk = qc_ket(qc);
     if (class_ms) JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));
     const int ge = c->grad_engine[qc];
-    if (ge == kEngineReg)
+    p.sides = ge == kGradEngineRegSplit ? 2 : 1;
+    if (grad_reg_engine(ge))
       JQC_CUDA_CHECK(launch_grad_reg(qc, p, s));
     else if (ge == kEngineCol)
       JQC_CUDA_CHECK(launch_grad_row(qc, p, s));
@@ -1341,8 +1348,9 @@ int jqc_set_grad_engine(jqc_ctx* c, int quartet_class, int engine) {
   JQC_REQUIRE(quartet_class >= 0 && quartet_class < kNumQuartetClasses, JQC_ERR_INVALID,
               "jqc_set_grad_engine: quartet class out of range");
   JQC_REQUIRE(grad_engine_valid(engine, quartet_class), JQC_ERR_INVALID,
-              "jqc_set_grad_engine: engine must be 0 (register, L <= 4), 1 (row, dp/dd bra) or 2 (warp)");
-  const bool per_task_changed = (c->grad_engine[quartet_class] == kEngineReg) != (engine == kEngineReg);
+              "jqc_set_grad_engine: engine must be 0 (register, L <= 4), 1 (row, dp/dd bra), 2 (warp) or "
+              "3 (register, bra and ket forces in separate parts, L <= 4)");
+  const bool per_task_changed = grad_reg_engine(c->grad_engine[quartet_class]) != grad_reg_engine(engine);
   c->grad_engine[quartet_class] = engine;
   if (per_task_changed && c->grad_tasks.valid) {
     drop_graphs(c);

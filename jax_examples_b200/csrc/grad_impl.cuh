@@ -43,14 +43,16 @@ struct GradBody {
   int warp, lane;
   GradBraSmem<LA, LB>* sb;
 
-  template <int PART>
+  // SIDE 0: all forces; 1: bra centres (A, B) only; 2: ket centre C only.
+  template <int PART, int SIDE = 0>
   __device__ __forceinline__ void run() {
     using Cfg = QCfg<LA, LB, LC, LD, NS, PART>;
-    if constexpr (Cfg::NCDP > 0) body<PART>();
+    if constexpr (Cfg::NCDP > 0) body<PART, SIDE>();
   }
 
-  template <int PART>
+  template <int PART, int SIDE>
   __device__ __forceinline__ void body() {
+    constexpr bool kBra = SIDE != 2, kKet = SIDE != 1;
     using Cfg = QCfg<LA, LB, LC, LD, NS, PART>;
     constexpr int NA = Cfg::NA, NB = Cfg::NB, ND = Cfg::ND;
     constexpr int NCDP = Cfg::NCDP;
@@ -136,6 +138,7 @@ struct GradBody {
           constexpr int cd = Cfg::CD0 + cdi, c = cd / ND, d = cd % ND;
           constexpr int cx = cart_lx(LC, c), cy = cart_ly(LC, c), cz = cart_lz(LC, c);
           constexpr int dx = cart_lx(LD, d), dy = cart_ly(LD, d), dz = cart_lz(LD, d);
+          if constexpr (kBra) {
           // stage 1 with one extra bra Hermite order
           double X[NH1];
           static_for<NH1>([&](auto h) { X[decltype(h)::value] = 0.0; });
@@ -206,8 +209,9 @@ struct GradBody {
             g[4] += w * s4;
             g[5] += w * s5;
           });
+          }
           // ket (centre C) derivative, one axis at a time
-          static_for<3>([&](auto dir_) {
+          if constexpr (kKet) static_for<3>([&](auto dir_) {
             constexpr int dir = decltype(dir_)::value;
             constexpr int ex = cx + dx + (dir == 0), ey = cy + dy + (dir == 1), ez = cz + dz + (dir == 2);
             double Xp[NH0];
@@ -276,37 +280,69 @@ struct GradBody {
     if (task.bra == kidx) sc *= 0.5;
     static_for<9>([&](auto k) { g[decltype(k)::value] *= sc; });
     double* pf = prm.pair_force;
-    static_for<6>([&](auto k_) {
-      constexpr int k = decltype(k_)::value;
-      const double v = warp_sum(g[k]);
-      if (lane == 0) atomicAdd(pf + 6 * task.bra + k, v);
-    });
+    if constexpr (kBra) {
+      static_for<6>([&](auto k_) {
+        constexpr int k = decltype(k_)::value;
+        const double v = warp_sum(g[k]);
+        if (lane == 0) atomicAdd(pf + 6 * task.bra + k, v);
+      });
+    }
+    // centre D by translational invariance: each side adds minus its own part
     if (active) {
       static_for<3>([&](auto k_) {
         constexpr int k = decltype(k_)::value;
-        atomicAdd(pf + 6 * kidx + k, g[6 + k]);
-        atomicAdd(pf + 6 * kidx + 3 + k, -(g[k] + g[3 + k] + g[6 + k]));
+        if constexpr (kKet) atomicAdd(pf + 6 * kidx + k, g[6 + k]);
+        atomicAdd(pf + 6 * kidx + 3 + k, -((kBra ? g[k] + g[3 + k] : 0.0) + (kKet ? g[6 + k] : 0.0)));
       });
     }
   }
 };
 
-template <int LA, int LB, int LC, int LD>
+// Runs one side of GradBody for the part dispatch_part selects.
+template <typename Body, int SIDE>
+struct GradSide {
+  Body& b;
+  template <int PART>
+  __device__ __forceinline__ void run() {
+    b.template run<PART, SIDE>();
+  }
+};
+
+// SIDES = 1: one block part per ket Cartesian part computes every force.
+// SIDES = 2: the bra-centre and the ket-centre forces run in separate block
+// parts (blockIdx.y = 2 * part + side), each with its own R and Boys values,
+// so a thread holds only the stage-1 sums of one side (the L = 3, 4 classes
+// otherwise spill kilobytes per thread).
+template <int LA, int LB, int LC, int LD, int SIDES>
 __global__ void __launch_bounds__(128) grad_kernel(const GradParams prm) {
   constexpr int NS = grad_split(LA, LB, LC, LD);
   __shared__ GradBraSmem<LA, LB> sB[4];
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= prm.n_tasks) return;
-  GradBody<LA, LB, LC, LD, NS> body{prm, warp, int(threadIdx.x & 31), &sB[threadIdx.x >> 5]};
-  dispatch_part<NS>(blockIdx.y, body);
+  using Body = GradBody<LA, LB, LC, LD, NS>;
+  Body body{prm, warp, int(threadIdx.x & 31), &sB[threadIdx.x >> 5]};
+  if constexpr (SIDES == 1) {
+    dispatch_part<NS>(blockIdx.y, body);
+  } else if (blockIdx.y & 1) {
+    GradSide<Body, 2> side{body};
+    dispatch_part<NS>(blockIdx.y >> 1, side);
+  } else {
+    GradSide<Body, 1> side{body};
+    dispatch_part<NS>(blockIdx.y >> 1, side);
+  }
 }
 
 template <int LA, int LB, int LC, int LD>
 cudaError_t launch_grad_class(const GradParams& p, cudaStream_t s) {
   constexpr int NS = grad_split(LA, LB, LC, LD);
   if (p.n_tasks == 0) return cudaSuccess;
-  dim3 grid((p.n_tasks + 3) / 4, NS);
-  grad_kernel<LA, LB, LC, LD><<<grid, 128, 0, s>>>(p);
+  if (p.sides == 2) {
+    dim3 grid((p.n_tasks + 3) / 4, 2 * NS);
+    grad_kernel<LA, LB, LC, LD, 2><<<grid, 128, 0, s>>>(p);
+  } else {
+    dim3 grid((p.n_tasks + 3) / 4, NS);
+    grad_kernel<LA, LB, LC, LD, 1><<<grid, 128, 0, s>>>(p);
+  }
   return cudaGetLastError();
 }
 

@@ -129,7 +129,12 @@ struct GradParams {
   const float* dmax = nullptr;  // n_shell x n_shell max |D^s| per shell block, or null
   int n_shell = 0;
   float dens_tau = 0.f;   // skip quartets whose Gamma bound x Q_ab Q_cd is below this
+  int sides = 1;          // register kernels: 2 = bra and ket forces in separate block parts
 };
+
+// Gradient engine code of the register kernels with the bra-centre and
+// ket-centre forces in separate block parts (GradParams::sides = 2).
+constexpr int kGradEngineRegSplit = 3;
 
 // Upper bound of |Gamma_abcd| over a shell quartet from the per-block density
 // maxima m (max over the n_dens densities): |D^t| <= n_dens m, so

@@ -270,8 +270,9 @@ def _set_grad_engines(eng, engine, classes):
 
 
 def test_gradient_engines_agree():
-    """The register, row and warp engines of the ERI-derivative adjoint give
-    the same two-electron gradient (1e-10 Eh/bohr) wherever they overlap."""
+    """The register (one or two sides), row and warp engines of the
+    ERI-derivative adjoint give the same two-electron gradient (1e-10
+    Eh/bohr) wherever they overlap."""
     from jax_examples_b200.grad import grad_two_electron
 
     mol = pb.water_cluster(3, seed=12, noise_angstrom=0.1)
@@ -294,8 +295,14 @@ def test_gradient_engines_agree():
     _set_grad_engines(eng, 0, [11, 15])  # register kernels for the L <= 4 row classes
     g_reg = grad_two_electron(eng, [D], 1.0, 0.5)
     np.testing.assert_allclose(g_reg.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
+    reg = [q for q in range(21) if q not in (12, 13, 14, 16, 17, 18, 19, 20)]
+    _set_grad_engines(eng, 3, reg)  # register kernels, bra and ket forces in separate parts
+    g_split = grad_two_electron(eng, [D], 1.0, 0.5)
+    np.testing.assert_allclose(g_split.cpu().numpy(), g0.cpu().numpy(), atol=1e-10, rtol=0)
     with pytest.raises(ValueError, match="engine"):
         _abi.call("jqc_set_grad_engine", eng._ctx, 0, 1)  # (ss|ss) has no row kernel
+    with pytest.raises(ValueError, match="engine"):
+        _abi.call("jqc_set_grad_engine", eng._ctx, 13, 3)  # (dp|ds): L = 5, no register kernel
     eng.close()
 
 
