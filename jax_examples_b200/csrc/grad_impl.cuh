@@ -101,7 +101,7 @@ struct GradBody {
 
     const int p0 = task.flags & 0xffff, p1 = task.flags >> 16;  // bra primitive-pair range
     for (int ip = p0; ip < p1; ++ip) {
-      const PrimPair bpp = prm.pp[bp.pp + ip];
+      const PrimPair bpp = ld_pp(prm.pp + bp.pp + ip);
       __syncwarp();
       if (lane < 3) {
         const double P = lane == 0 ? bpp.Px : lane == 1 ? bpp.Py : bpp.Pz;
@@ -124,7 +124,7 @@ struct GradBody {
       }
       __syncwarp();
       for (int iq = 0; iq < nket; ++iq) {
-        const PrimPair kpp = prm.pp[kp.pp + iq];
+        const PrimPair kpp = ld_pp(prm.pp + kp.pp + iq);
         double F[3][LC + 2][LD + 1][LC + LD + 2];
         ecoef_compute<double, LC + 1, LD, true>(F[0], kpp.Px - C.x, kpp.Px - Dc.x, kpp.h);
         ecoef_compute<double, LC + 1, LD, true>(F[1], kpp.Py - C.y, kpp.Py - Dc.y, kpp.h);
