@@ -258,10 +258,12 @@ class _BatchFock:
       mixed build (FP32 for Q_ij Q_kl < mixed_tau); then each build contracts
       the density change of the active molecules (J, K are linear in D) with
       density screening at ``mixed_dens_tau``, a full rebuild every
-      ``rebuild_every`` builds.  Once the largest DIIS error of the active
-      molecules is below ``fp64_switch`` it switches to a full FP64 build and
-      incremental FP64 builds screened at ``fp64_tail_dens_tau``; convergence
-      is accepted only after ``fp64_tail_iters`` FP64 builds.
+      ``rebuild_every`` builds (full mixed builds screened at
+      ``mixed_full_dens_tau``).  Once the largest DIIS error of the active
+      molecules is below ``fp64_switch`` it switches to a full FP64 build
+      (screened at ``fp64_switch_dens_tau``) and incremental FP64 builds
+      screened at ``fp64_tail_dens_tau``; convergence is accepted only after
+      ``fp64_tail_iters`` FP64 builds.
     """
 
     def __init__(self, eng: BatchedERI, batch: MoleculeBatch, config: CalcConfig, use_graph: bool,
@@ -285,10 +287,17 @@ class _BatchFock:
         self.Jacc = torch.zeros_like(self.J[0])
         self.Kacc = torch.zeros_like(self.K[0])
 
-    def _settings(self, incremental: bool):
-        if self.phase == "mixed":
-            return "mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU) if incremental else BATCH_DENS_TAU
-        return "fp64", self.tail_tau if incremental else BATCH_DENS_TAU
+    def _settings(self, incremental: bool, phase: Optional[str] = None):
+        """(precision, density-screening threshold) of the next build."""
+        phase = self.phase if phase is None else phase
+        if phase == "mixed":
+            tau = self.config.mixed_dens_tau if incremental else self.config.mixed_full_dens_tau
+            return "mixed", max(float(tau), BATCH_DENS_TAU)
+        if not self.mixed:
+            return "fp64", BATCH_DENS_TAU  # plain FP64: unscreened apart from zero blocks
+        if incremental:
+            return "fp64", self.tail_tau
+        return "fp64", max(float(self.config.fp64_switch_dens_tau), BATCH_DENS_TAU)
 
     def _launch(self, incremental: bool):
         prec, tau = self._settings(incremental)
@@ -322,9 +331,9 @@ class _BatchFock:
         if self.use_graph:
             kinds = [(prec, tau)]
             if self.mixed:
-                kinds += [("fp64", BATCH_DENS_TAU)]
+                kinds += [self._settings(False, "fp64")]
             if self.incremental:
-                kinds += [("mixed", max(float(self.config.mixed_dens_tau), BATCH_DENS_TAU)), ("fp64", self.tail_tau)]
+                kinds += [self._settings(True, "mixed"), self._settings(True, "fp64")]
             t0 = time.perf_counter()
             for p_, t_ in kinds:
                 self.graphs[(p_, t_)] = self.eng.capture_jk(self.D, self.J, self.K, p_, self.mixed_tau, t_)

@@ -142,7 +142,16 @@ class CalcConfig(_Replace):
                     in the mixed phase.
     fp64_tail_dens_tau: density-screening threshold of the incremental FP64
                     builds after the switch (mixed mode only; plain FP64
-                    incremental builds screen at 1e-12).
+                    incremental builds screen at 1e-12).  1e-11: at 1e-10 the
+                    64-cluster sweep's largest energy error reached 7.6e-7 Eh
+                    (3.0e-7 at 1e-12, with no slower Fock builds there).
+    mixed_full_dens_tau: density-screening threshold of the full builds of
+                    the mixed phase (their errors are dropped at the switch).
+    fp64_switch_dens_tau: density-screening threshold of the full FP64 build
+                    at the switch (mixed mode only; plain FP64 builds are
+                    unscreened).  0: 1e-11 saves ~1 ms on (H2O)16 but moved
+                    the 64-cluster sweep's largest energy error from about
+                    6.5e-7 to 7.1e-7 Eh, too close to the 1e-6 tolerance.
     """
 
     method: str = "rhf"
@@ -162,7 +171,9 @@ class CalcConfig(_Replace):
     fp64_switch: float = 1e-5
     incremental: bool = True
     mixed_dens_tau: float = 1e-8
-    fp64_tail_dens_tau: float = 1e-10
+    fp64_tail_dens_tau: float = 1e-11
+    mixed_full_dens_tau: float = 1e-9
+    fp64_switch_dens_tau: float = 0.0
 
 
 def make_molecule(elements, coords, atomic_numbers, charge: int = 0, spin: int = 0) -> Molecule:
