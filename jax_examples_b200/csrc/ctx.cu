@@ -1178,6 +1178,7 @@ int jqc_grad1e(jqc_ctx* c, const double* D, const double* W, double* grad, void*
   p.shell_mol = c->n_mol > 1 ? c->d_shell_mol.ptr : nullptr;
   p.atom_mol = c->n_mol > 1 ? c->d_atom_mol.ptr : nullptr;
   p.boys = c->boys64;
+  p.boys_al = c->boysA64;
   p.D = D;
   p.W = W;
   p.grad = grad;

@@ -391,234 +391,5 @@ cudaError_t launch_warp_grad(int la, int lb, int lc, int ld, const GradParams& p
   return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------
-// One-electron derivative terms over shell pairs (a >= b):
-//   grad += sum_ab D_ab d(T+V)_ab/dR - W_ab dS_ab/dR
-// with d/dA from derivative E coefficients (A-side 2 alpha E_{i+1} - i E_{i-1}),
-// d/dB = -d/dA for S and T, and per nucleus C of V the operator-centre term
-// dV/dC_x = -Z_C (2 pi/p) K sum E E E (-R_{t+1,u,v}) (Hellmann-Feynman) with
-// dV/dB = -dV/dA - dV/dC.
-// Shared set-up of one primitive pair: Gaussian product and the per-axis E
-// coefficients up to (la+2, lb+1) (enough for kinetic-energy derivatives).
-struct Prim1 {
-  double al, be, pp, K, P[3];
-  double E[3][5][4][8];
-};
-
-__device__ void prim1_setup(Prim1& q, double al, double be, double w, const double* A, const double* B, int la,
-                            int lb) {
-  q.al = al;
-  q.be = be;
-  q.pp = al + be;
-  const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
-  for (int x = 0; x < 3; ++x) q.P[x] = (al * A[x] + be * B[x]) / q.pp;
-  q.K = exp(-(al * be / q.pp) * ab2) * w;
-  const double inv2p = 0.5 / q.pp;
-  for (int x = 0; x < 3; ++x) {
-    const double pa = q.P[x] - A[x], pb = q.P[x] - B[x];
-    for (int a = 0; a <= la + 2; ++a)
-      for (int b = 0; b <= lb + 1; ++b)
-        for (int tt = 0; tt < 8; ++tt) q.E[x][a][b][tt] = 0.0;
-    q.E[x][0][0][0] = 1.0;
-    for (int a = 0; a < la + 2; ++a)
-      for (int tt = 0; tt <= a + 1; ++tt) {
-        double val = 0.0;
-        if (tt <= a) val = pa * q.E[x][a][0][tt];
-        if (tt >= 1) val += inv2p * q.E[x][a][0][tt - 1];
-        if (tt + 1 <= a) val += (tt + 1) * q.E[x][a][0][tt + 1];
-        q.E[x][a + 1][0][tt] = val;
-      }
-    for (int b = 0; b < lb + 1; ++b)
-      for (int a = 0; a <= la + 2; ++a)
-        for (int tt = 0; tt <= a + b + 1; ++tt) {
-          double val = 0.0;
-          if (tt <= a + b) val = pb * q.E[x][a][b][tt];
-          if (tt >= 1) val += inv2p * q.E[x][a][b][tt - 1];
-          if (tt + 1 <= a + b) val += (tt + 1) * q.E[x][a][b][tt + 1];
-          q.E[x][a][b + 1][tt] = val;
-        }
-  }
-}
-
-__device__ __forceinline__ void pair_index(int idx, int& i, int& j) {
-  i = (int)((sqrt(8.0 * idx + 1.0) - 1.0) * 0.5);
-  while (i * (i + 1) / 2 > idx) --i;
-  while ((i + 1) * (i + 2) / 2 <= idx) ++i;
-  j = idx - i * (i + 1) / 2;
-}
-
-// Overlap and kinetic parts: one thread per shell pair.  d/dB = -d/dA.
-__global__ void grad1e_st_kernel(const Grad1Params p) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int npair = p.n_shell * (p.n_shell + 1) / 2;
-  if (idx >= npair) return;
-  int i, j;
-  pair_index(idx, i, j);
-  if (p.shell_mol && p.shell_mol[i] != p.shell_mol[j]) return;  // shells of two molecules of a batch
-  const double fac = (i == j) ? 1.0 : 2.0;
-  const int la = p.l[i], lb = p.l[j];
-  const int na = ncart(la), nb = ncart(lb);
-  const double* A = p.centres + 3 * i;
-  const double* B = p.centres + 3 * j;
-  const int a0 = p.ao[i], b0 = p.ao[j];
-  double gA[3] = {0, 0, 0};
-  Prim1 q;
-  for (int ia = 0; ia < p.nprim[i]; ++ia)
-    for (int ib = 0; ib < p.nprim[j]; ++ib) {
-      prim1_setup(q, p.exps[p.prim_off[i] + ia], p.exps[p.prim_off[j] + ib],
-                  p.coefs[p.prim_off[i] + ia] * p.coefs[p.prim_off[j] + ib], A, B, la, lb);
-      const double al = q.al, be = q.be;
-      double S1[3][5][4], T1[3][4][3];
-      const double sq = sqrt(M_PI / q.pp);
-      for (int x = 0; x < 3; ++x) {
-        for (int a = 0; a <= la + 2; ++a)
-          for (int b = 0; b <= lb + 1; ++b) S1[x][a][b] = sq * q.E[x][a][b][0];
-        for (int a = 0; a <= la + 1; ++a)
-          for (int b = 0; b <= lb; ++b) {
-            double tv = 4.0 * al * be * S1[x][a + 1][b + 1];
-            if (a > 0 && b > 0) tv += a * b * S1[x][a - 1][b - 1];
-            if (b > 0) tv -= 2.0 * al * b * S1[x][a + 1][b - 1];
-            if (a > 0) tv -= 2.0 * be * a * S1[x][a - 1][b + 1];
-            T1[x][a][b] = 0.5 * tv;
-          }
-      }
-      for (int a = 0; a < na; ++a)
-        for (int b = 0; b < nb; ++b) {
-          int ac[3], bc[3];
-          wcart(la, a, ac[0], ac[1], ac[2]);
-          wcart(lb, b, bc[0], bc[1], bc[2]);
-          const double dv = p.D[(size_t)(a0 + a) * p.n + b0 + b];
-          const double wv = p.W[(size_t)(a0 + a) * p.n + b0 + b];
-          double s[3], tk[3], ds[3], dt[3];
-          for (int x = 0; x < 3; ++x) {
-            s[x] = S1[x][ac[x]][bc[x]];
-            tk[x] = T1[x][ac[x]][bc[x]];
-            ds[x] = 2.0 * al * S1[x][ac[x] + 1][bc[x]] - (ac[x] > 0 ? ac[x] * S1[x][ac[x] - 1][bc[x]] : 0.0);
-            dt[x] = 2.0 * al * T1[x][ac[x] + 1][bc[x]] - (ac[x] > 0 ? ac[x] * T1[x][ac[x] - 1][bc[x]] : 0.0);
-          }
-          for (int x = 0; x < 3; ++x) {
-            const int y = (x + 1) % 3, z = (x + 2) % 3;
-            const double dS = q.K * ds[x] * s[y] * s[z];
-            const double dT = q.K * (dt[x] * s[y] * s[z] + ds[x] * (tk[y] * s[z] + s[y] * tk[z]));
-            gA[x] += dv * dT - wv * dS;
-          }
-        }
-    }
-  const int atA = p.atom[i], atB = p.atom[j];
-  for (int x = 0; x < 3; ++x) {
-    atomicAdd(p.grad + 3 * atA + x, fac * gA[x]);
-    atomicAdd(p.grad + 3 * atB + x, -fac * gA[x]);
-  }
-}
-
-// Nuclear attraction of one nucleus C: one thread per (shell pair, nucleus).
-// d/dA from derivative E coefficients, d/dC (Hellmann-Feynman) from
-// dR_tuv/dC_x = -R_{t+1,u,v}, and d/dB = -d/dA - d/dC.
-__global__ void grad1e_v_kernel(const Grad1Params p) {
-  const long long gidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long npair = (long long)p.n_shell * (p.n_shell + 1) / 2;
-  if (gidx >= npair * p.n_atom) return;
-  const int idx = (int)(gidx / p.n_atom), c = (int)(gidx % p.n_atom);
-  int i, j;
-  pair_index(idx, i, j);
-  // batch: the pair and the nucleus belong to one molecule
-  if (p.shell_mol && (p.shell_mol[i] != p.shell_mol[j] || p.atom_mol[c] != p.shell_mol[i])) return;
-  const double fac = (i == j) ? 1.0 : 2.0;
-  const int la = p.l[i], lb = p.l[j];
-  const int na = ncart(la), nb = ncart(lb);
-  const double* A = p.centres + 3 * i;
-  const double* B = p.centres + 3 * j;
-  const int a0 = p.ao[i], b0 = p.ao[j];
-  double gA[3] = {0, 0, 0}, gC[3] = {0, 0, 0};
-  Prim1 q;
-  for (int ia = 0; ia < p.nprim[i]; ++ia)
-    for (int ib = 0; ib < p.nprim[j]; ++ib) {
-      prim1_setup(q, p.exps[p.prim_off[i] + ia], p.exps[p.prim_off[j] + ib],
-                  p.coefs[p.prim_off[i] + ia] * p.coefs[p.prim_off[j] + ib], A, B, la, lb);
-      const double al = q.al, pp = q.pp;
-      const int L = la + lb + 1;
-      const double X = q.P[0] - p.atom_xyz[3 * c], Y = q.P[1] - p.atom_xyz[3 * c + 1],
-                   Z = q.P[2] - p.atom_xyz[3 * c + 2];
-      double F[kBoysMaxM + 1];
-      boys_eval_rt<double>(pp * (X * X + Y * Y + Z * Z), p.boys, L, F);
-      const double pref = -p.atom_Z[c] * (2.0 * M_PI / pp) * q.K;
-      double R[nherm(5)];
-      double Rn[6];
-      double pw = pref;
-      for (int m = 0; m <= L; ++m) {
-        Rn[m] = pw * F[m];
-        pw *= -2.0 * pp;
-      }
-      R[0] = Rn[L];
-      for (int m = L - 1; m >= 0; --m) {
-        for (int sh = L - m; sh >= 1; --sh) {
-          const int base = sh * (sh + 1) * (sh + 2) / 6;
-          for (int k = 0; k < ncart(sh); ++k) {
-            int tt, u, vv;
-            wcart(sh, k, tt, u, vv);
-            double val;
-            if (tt > 0) {
-              val = X * R[herm_index(tt - 1, u, vv)];
-              if (tt > 1) val += (tt - 1) * R[herm_index(tt - 2, u, vv)];
-            } else if (u > 0) {
-              val = Y * R[herm_index(tt, u - 1, vv)];
-              if (u > 1) val += (u - 1) * R[herm_index(tt, u - 2, vv)];
-            } else {
-              val = Z * R[herm_index(tt, u, vv - 1)];
-              if (vv > 1) val += (vv - 1) * R[herm_index(tt, u, vv - 2)];
-            }
-            R[base + k] = val;
-          }
-        }
-        R[0] = Rn[m];
-      }
-      for (int a = 0; a < na; ++a)
-        for (int b = 0; b < nb; ++b) {
-          int ac[3], bc[3];
-          wcart(la, a, ac[0], ac[1], ac[2]);
-          wcart(lb, b, bc[0], bc[1], bc[2]);
-          const double dv = p.D[(size_t)(a0 + a) * p.n + b0 + b];
-          for (int x = 0; x < 3; ++x) {
-            const int y = (x + 1) % 3, z = (x + 2) % 3;
-            double accA = 0.0, accC = 0.0;
-            for (int t0 = 0; t0 <= ac[x] + bc[x] + 1; ++t0) {
-              double de = 2.0 * al * q.E[x][ac[x] + 1][bc[x]][t0];
-              if (ac[x] > 0) de -= ac[x] * q.E[x][ac[x] - 1][bc[x]][t0];
-              const double e0 = t0 <= ac[x] + bc[x] ? q.E[x][ac[x]][bc[x]][t0] : 0.0;
-              for (int u0 = 0; u0 <= ac[y] + bc[y]; ++u0)
-                for (int v0 = 0; v0 <= ac[z] + bc[z]; ++v0) {
-                  int h[3];
-                  h[x] = t0;
-                  h[y] = u0;
-                  h[z] = v0;
-                  const double eyz = q.E[y][ac[y]][bc[y]][u0] * q.E[z][ac[z]][bc[z]][v0];
-                  accA += de * eyz * R[herm_index(h[0], h[1], h[2])];
-                  if (t0 <= ac[x] + bc[x]) {
-                    h[x] += 1;
-                    accC -= e0 * eyz * R[herm_index(h[0], h[1], h[2])];
-                  }
-                }
-            }
-            gA[x] += dv * accA;
-            gC[x] += dv * accC;
-          }
-        }
-    }
-  const int atA = p.atom[i], atB = p.atom[j];
-  for (int x = 0; x < 3; ++x) {
-    atomicAdd(p.grad + 3 * atA + x, fac * gA[x]);
-    atomicAdd(p.grad + 3 * c + x, fac * gC[x]);
-    atomicAdd(p.grad + 3 * atB + x, -fac * (gA[x] + gC[x]));
-  }
-}
-
-cudaError_t launch_grad1e(const Grad1Params& p, cudaStream_t s) {
-  const long long npair = (long long)p.n_shell * (p.n_shell + 1) / 2;
-  if (npair == 0) return cudaSuccess;
-  grad1e_st_kernel<<<(unsigned)((npair + 63) / 64), 64, 0, s>>>(p);
-  const long long nv = npair * p.n_atom;
-  if (nv > 0) grad1e_v_kernel<<<(unsigned)((nv + 63) / 64), 64, 0, s>>>(p);
-  return cudaGetLastError();
-}
 
 }  // namespace jqc

@@ -162,6 +162,7 @@ struct Grad1Params {
   const int* shell_mol;  // molecule of each shell / atom (nullptr: one molecule)
   const int* atom_mol;
   const double* boys;
+  const double* boys_al;  // aligned per-order Boys table
   const double* D;
   const double* W;
   double* grad;
