@@ -281,6 +281,7 @@ class _BatchFock:
         self.since_full = 0
         self.prev = None  # densities of the last build, per molecule
         self.events = []
+        self.kinds = []  # (kind, active molecules) of every build
         self.graphs = {}
         self.log = {"builds_mixed": 0, "builds_fp64": 0, "incremental_builds": 0}
         self.D, self.J, self.K = eng.buffers(1)
@@ -378,6 +379,7 @@ class _BatchFock:
             self.prev = dict(dens)
         e1.record()
         self.events.append((e0, e1))
+        self.kinds.append(("%s-%s" % (self._settings(inc)[0], "inc" if inc else "full"), len(dens)))
         return {m: (b.block(self.Jacc, m), b.block(self.Kacc, m)) for m in dens}
 
     def observe(self, err_max: float) -> None:
@@ -393,6 +395,13 @@ class _BatchFock:
             return 0.0
         self.events[-1][1].synchronize()
         return sum(a.elapsed_time(c) for a, c in self.events) * 1e-3
+
+    def build_ms(self) -> list:
+        """[kind, active molecules, milliseconds] of every build."""
+        if not self.events:
+            return []
+        self.events[-1][1].synchronize()
+        return [[k, n, round(a.elapsed_time(c), 3)] for (k, n), (a, c) in zip(self.kinds, self.events)]
 
 
 _HOST_EIGH_MAX_N = 512
@@ -572,7 +581,8 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
         for g in groups:
             g.active = torch.tensor([not converged[m] for m in g.members], device=g.D.device)
     record = dict(fb.log, fock_builds=sum(fb.log[k] for k in ("builds_mixed", "builds_fp64")),
-                  jk_seconds=fb.seconds(), setup_seconds=setup_s, graph=bool(fb.graphs), autotuned=bool(autotune),
+                  jk_seconds=fb.seconds(), build_ms=fb.build_ms(), setup_seconds=setup_s, graph=bool(fb.graphs),
+                  autotuned=bool(autotune),
                   n_molecules=M, n_basis=batch.n_basis, precision=config.precision,
                   incremental=fb.incremental, groups=len(groups), prepare_seconds=prepare_s,
                   prepare_breakdown=getattr(fb, "prep_times", {}))
