@@ -12,7 +12,7 @@ the precision policy of the mixed path:
   (FP64 accumulation), and with ``incremental=True`` each build contracts only
   the density change dD = D - D_prev (J, K are linear in D) with density-
   weighted screening, the error of which is reset by a full rebuild every
-  ``rebuild_every`` builds (itself screened at ``mixed_full_dens_tau``, 1e-9:
+  ``rebuild_every`` builds of the mixed phase (itself screened at ``mixed_full_dens_tau``, 1e-9:
   8.3 -> 5.6 ms on (H2O)16 with the same iterations and final error).  In
   this phase the incremental builds screen at
   ``mixed_dens_tau`` (1e-8: the early Fock matrices only steer the next
@@ -135,7 +135,10 @@ class FockBuilder:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        use_inc = self.incremental and self._prev is not None and self._since_full < self.rebuild_every
+        # periodic rebuilds in the mixed phase (and on the plain incremental
+        # path); the FP64 tail of the mixed policy has none
+        tail = self.precision == "mixed" and prec == "fp64"
+        use_inc = self.incremental and self._prev is not None and (tail or self._since_full < self.rebuild_every)
         if use_inc and self._prev[0].shape == D.shape:
             dD = D - self._prev[0]
             if prec == "mixed":
