@@ -1,7 +1,7 @@
 """Benchmark of the two-electron hot path on B200.
 
 Workload: (H2O)_16 on the 2.9 A cubic lattice with seeded rotations,
-6-31G*-shaped Cartesian basis (304 functions, 160 shells), Schwarz
+6-31G* Cartesian basis (304 functions, 160 shells), Schwarz
 threshold 1e-12.  One step = one direct FP64 J/K Fock build (fused MMD ERI +
 J/K digestion, the plain kernel) from the core-guess density.
 
@@ -31,6 +31,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -39,14 +40,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_WATERS = int(os.environ.get("JQC_BENCH_WATERS", "16"))
-BASIS = "syn-6-31g*"
+BASIS = "6-31g*"
 SCHWARZ_TAU = 1e-12
 # density-screening threshold of the chosen (mixed) path's gradient (the
 # batched path's MIXED_GRAD_TAU): skipped quartets change the (H2O)16
 # gradient by ~3.5e-6 Eh/bohr, inside the 1e-5 tolerance of the mixed path
 CHOSEN_GRAD_TAU = 3e-10
-METRIC = "ERI quartets/s (direct J/K Fock build, (H2O)16 6-31G*-shaped)"
-WORKLOAD = (f"(H2O){N_WATERS} lattice 2.9A, 6-31G*-shaped Cartesian ({19 * N_WATERS} bf), "
+METRIC = "ERI quartets/s (direct J/K Fock build, (H2O)16 6-31G*)"
+WORKLOAD = (f"(H2O){N_WATERS} lattice 2.9A, 6-31G* Cartesian ({19 * N_WATERS} bf), "
             "FP64 direct J/K build")
 
 
@@ -252,6 +253,150 @@ def batched_sweep(local: int, n_mol: int, seed: int = 2024):
     }
 
 
+def config3_scf(local: int, split_tau: float = 1e-7):
+    """(H2O)8 on the lattice, 6-31G* Cartesian (152 bf): RHF-DIIS to 1e-8 Eh
+    with the plain FP64 build every iteration against the mixed build with
+    the FP32/FP64 Schwarz split at ``split_tau`` (and the package's default
+    split beside it); iterations, Fock seconds and the energy error against
+    FP64.  The same FP64 SCF in 6-31G** (200 bf) gives that basis's size and
+    time."""
+    import torch
+
+    from jax_examples_b200 import CalcConfig, compute_integrals, run_scf
+    from jax_examples_b200 import basis as pb
+
+    mol = pb.water_cluster(8, seed=0)
+    out = {"workload": "(H2O)8 lattice 2.9A, RHF-DIIS to 1e-8 Eh, Schwarz 1e-12"}
+    for basis in ("6-31g*", "6-31g**"):
+        bs = pb.build_basis_set(mol, basis)
+        ints = compute_integrals(mol, bs, device=local, schwarz_tau=SCHWARZ_TAU)
+        runs = [("fp64", CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU, incremental=False))]
+        if basis == "6-31g*":
+            runs += [(f"mixed_split_{split_tau:g}", CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU,
+                                                             precision="mixed", mixed_tau=split_tau)),
+                     ("mixed_default", CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU, precision="mixed"))]
+        rows = {}
+        for name, cfg in runs:
+            run_scf(mol, ints, cfg)  # warm-up: work lists built, kernels loaded
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r = run_scf(mol, ints, cfg)
+            torch.cuda.synchronize()
+            rows[name] = {"energy": r.energy, "iterations": r.n_iterations, "converged": r.converged,
+                          "fock_s": round(r.precision["jk_seconds"], 4), "scf_s": round(time.perf_counter() - t0, 4),
+                          "mixed_tau": cfg.mixed_tau if cfg.precision == "mixed" else None}
+        e64 = rows["fp64"]["energy"]
+        for name, row in rows.items():
+            if name != "fp64":
+                row["energy_err_eh"] = abs(row["energy"] - e64)
+                row["fock_speedup"] = round(rows["fp64"]["fock_s"] / max(1e-12, row["fock_s"]), 3)
+        out[basis] = dict(rows, n_bf=bs.n_basis)
+        ints.ERI.close()
+    return out
+
+
+def _sequential_bfgs(local, mols, max_steps):
+    """The reference's loop shape on the device: one molecule at a time, every
+    BFGS evaluation a new engine, a plain FP64 SCF (full build every
+    iteration) and the unscreened analytic gradient
+    (geomopt/optimizer.py:55-76 per trial geometry)."""
+    from jax_examples_b200 import CalcConfig, DirectERI, compute_integrals, run_scf
+    from jax_examples_b200 import basis as pb
+    from jax_examples_b200.batch import _bfgs_walker
+    from jax_examples_b200.core import make_molecule
+    from jax_examples_b200.grad import rhf_gradient
+
+    cfg = CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU, incremental=False, max_scf_iter=200)
+    out, evals = [], 0
+    for mol in mols:
+        w = _bfgs_walker(mol, max_steps, 1e-4, 1e-6, 0.3)
+        xyz = w.send(None)
+        while True:
+            m = make_molecule(mol.elements, xyz, mol.atomic_numbers, charge=mol.charge, spin=mol.spin)
+            bs = pb.build_basis_set(m, BASIS)
+            eng = DirectERI(bs, m, device=local, schwarz_tau=SCHWARZ_TAU)
+            r = run_scf(m, compute_integrals(m, bs, device=local, engine=eng), cfg)
+            g = rhf_gradient(m, r, engine=eng).cpu().numpy()
+            eng.close()
+            evals += 1
+            try:
+                xyz = w.send((r.energy, g))
+            except StopIteration as stop:
+                out.append(stop.value)
+                break
+    return out, evals
+
+
+def batched_bfgs(local: int, n_mol: int, steps: int = 10, seed: int = 2024, seq_every: int = 4):
+    """The sweep's molecules (n_mol water clusters, 1..12 waters, +-0.1 A
+    noise) optimised for ``steps`` BFGS steps each on the batched path: one
+    engine for the whole optimisation, autotuned once, geometry-only updates
+    between rounds, mixed precision with incremental builds, screened
+    gradient.  Per-molecule energy and gradient error against FP64 at the
+    final geometries (one batched plain-FP64 evaluation there).  Every
+    ``seq_every``-th molecule is also optimised on the reference's loop shape
+    (one molecule and one new engine per evaluation, plain FP64) and on the
+    batched path alone, for the wall-clock comparison on the same subset."""
+    import torch
+
+    from jax_examples_b200 import CalcConfig
+    from jax_examples_b200 import basis as pb
+    from jax_examples_b200.batch import _BatchEvaluator, optimize_bfgs_batch
+
+    rng = np.random.default_rng(seed)
+    sizes = [int(x) for x in rng.integers(1, 13, n_mol)]
+    mols = [pb.water_cluster(n, seed=seed + i, noise_angstrom=0.1) for i, n in enumerate(sizes)]
+    chosen = CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU, precision="mixed", incremental=True,
+                        max_scf_iter=200)
+    plain = CalcConfig(scf_conv=1e-8, schwarz_tau=SCHWARZ_TAU, incremental=False, max_scf_iter=200)
+
+    def run_batched(ms):
+        tm = {}
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = optimize_bfgs_batch(ms, BASIS, max_steps=steps, config=chosen, autotune=True, timing=tm)
+        torch.cuda.synchronize()
+        return res, tm, time.perf_counter() - t0
+
+    res, tm, wall = run_batched(mols)
+    # FP64 at the final geometries: one batched plain evaluation
+    ev = _BatchEvaluator([r.molecule for r in res], BASIS, plain)
+    try:
+        ref = ev({i: np.asarray(r.molecule.coords) for i, r in enumerate(res)})
+    finally:
+        ev.close()
+    e_err = [abs(r.energy - ref[i][0]) for i, r in enumerate(res)]
+    g_err = [float(np.abs(np.asarray(r.gradient) - ref[i][1]).max()) for i, r in enumerate(res)]
+    sub = mols[::seq_every]
+    sub_res, sub_tm, sub_wall = run_batched(sub)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seq_res, seq_evals = _sequential_bfgs(local, sub, steps)
+    torch.cuda.synchronize()
+    seq_wall = time.perf_counter() - t0
+    traj_de = max(abs(a.energy - b.energy) for a, b in zip(sub_res, seq_res))
+    return {
+        "workload": f"{n_mol} water clusters, 1..12 waters (seeded), +-0.1 A noise, {BASIS}, {steps} BFGS steps each",
+        "bfgs_steps": steps,
+        "batched_mixed": {"wall_s": round(wall, 3), "rounds": tm.get("rounds"), "evaluations": tm.get("evaluations"),
+                          "fock_s": round(tm.get("jk_seconds", 0.0), 3),
+                          "gradient_s": round(tm.get("grad_seconds", 0.0), 3),
+                          "fock_builds": tm.get("fock_builds"),
+                          "setup_s": round(tm.get("setup_seconds", 0.0), 3),
+                          "setup_breakdown_s": {k: round(v, 3) for k, v in tm.get("prepare_breakdown", {}).items()},
+                          "geometry_update_s": round(tm.get("geometry_update_seconds", 0.0), 3),
+                          "steps_taken": [r.n_steps for r in res], "converged": sum(bool(r.converged) for r in res)},
+        "max_energy_err_vs_fp64_eh": max(e_err), "max_gradient_err_vs_fp64_eh_bohr": max(g_err),
+        "per_molecule_energy_err_eh": [float("%.3g" % x) for x in e_err],
+        "per_molecule_gradient_err_eh_bohr": [float("%.3g" % x) for x in g_err],
+        "subset": {"molecules": len(sub), "every": seq_every,
+                   "batched_wall_s": round(sub_wall, 3), "batched_evaluations": sub_tm.get("evaluations"),
+                   "sequential_fp64_wall_s": round(seq_wall, 3), "sequential_evaluations": seq_evals,
+                   "wall_speedup": round(seq_wall / max(1e-12, sub_wall), 3),
+                   "max_final_energy_diff_eh": traj_de},
+    }
+
+
 def kernel_configs(local: int):
     """The kernel-level configurations beside the Fock build: Boys
     throughput (2^24 T, half U[0,30], half log-U[1e-8,1e3], m = 0..8, FP64
@@ -306,14 +451,14 @@ def kernel_configs(local: int):
         torch.cuda.empty_cache()
     out["prim_quartets"] = prim
     h2o8 = {}
-    for basis in ("syn-6-31g*", "syn-6-31g**"):
+    for basis in ("6-31g*", "6-31g**"):
         mol = pb.water_cluster(8, seed=0)
         bs = pb.build_basis_set(mol, basis)
         eng = DirectERI(bs, mol, device=local, schwarz_tau=SCHWARZ_TAU)
         D = torch.eye(bs.n_basis, dtype=torch.float64, device=dev) * 0.1
         row = {"n_bf": bs.n_basis, "quartets": eng.stats("fp64")["quartets_fp64"]}
         row["fp64_ms"] = round(timed(lambda: eng.jk(D)) * 1e3, 3)
-        if basis == "syn-6-31g*":
+        if basis == "6-31g*":
             eng.stats("mixed", 1e-7)
             row["mixed_ms"] = round(timed(lambda: eng.jk(D, precision="mixed", mixed_tau=1e-7)) * 1e3, 3)
         h2o8[basis] = row
@@ -407,8 +552,8 @@ def run_ours(args):
     barrier()
     # --- device-timed region: K steps, L2 flushed before each
     times = []
-    clk = Clocks(os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv") if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else f"/tmp/jqc_clocks_{rank}.csv")
+    clk = Clocks(args.clock_log.format(rank=rank) if args.clock_log else
+                 os.path.join(tempfile.gettempdir(), f"jqc_clocks_{os.getpid()}_{rank}.csv"))
     with clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -545,6 +690,10 @@ def run_ours(args):
     sweep = None
     if world == 1 and args.batch_molecules > 0:
         sweep = batched_sweep(local, args.batch_molecules)
+    bfgs = None
+    if world == 1 and args.batch_molecules > 0 and args.bfgs_steps > 0:
+        bfgs = batched_bfgs(local, args.batch_molecules, args.bfgs_steps)
+    conf3 = config3_scf(local) if (world == 1 and args.scf) else None
     kconf = kernel_configs(local) if (world == 1 and args.kernel_configs) else None
 
     cpu = None
@@ -578,6 +727,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "fock_gradient": fg,
         "batched_sweep": sweep,
+        "batched_bfgs": bfgs,
+        "config3_scf": conf3,
         "kernel_configs": kconf,
     }
     print(json.dumps(line), flush=True)
@@ -598,9 +749,14 @@ def main():
     ap.add_argument("--no-scf", dest="scf", action="store_false")
     ap.add_argument("--batch-molecules", type=int, default=64,
                     help="molecules in the batched uneven-size sweep (0 skips it)")
+    ap.add_argument("--bfgs-steps", type=int, default=10,
+                    help="BFGS steps per molecule of the batched sweep (0 skips the optimisation leg)")
     ap.add_argument("--waters", type=int, default=None, help="cluster size (default 16; profiling uses smaller)")
     ap.add_argument("--no-kernel-configs", dest="kernel_configs", action="store_false",
                     help="skip the Boys / primitive-quartet / (H2O)8 kernel sections")
+    ap.add_argument("--clock-log", default=None,
+                    help="CSV file for the nvidia-smi clock samples of the timed region ({rank} is replaced; "
+                         "default: a temporary file)")
     ap.add_argument("--gradient-only", action="store_true",
                     help="time only the ERI-derivative adjoint (profiling case)")
     args = ap.parse_args()

@@ -78,6 +78,23 @@ int jqc_pairs_build(jqc_ctx *ctx, double schwarz_tau, double prim_tau, void *str
  * molecules is one call per step instead of one per molecule. */
 int jqc_batch_partition(jqc_ctx *ctx, int n_mol, const int *mol_of_atom);
 
+/* Geometry-only update: atom a moves to atom_xyz[3a..3a+2] (bohr) and every
+ * shell of atom a with it; exponents, contractions, the batch partition, the
+ * molecule mask, launch tuning and the Boys tables stay.  The pair list, work
+ * lists and captured graphs are dropped: call jqc_pairs_build before the
+ * next J/K, gradient or one-electron call.  Replaces the per-step rebuild of
+ * geomopt/optimizer.py:55-76 (_energy_and_gradient builds the basis and all
+ * integrals anew for every trial geometry). */
+int jqc_set_geometry(jqc_ctx *ctx, const double *atom_xyz);
+
+/* Molecules taking part in the next jqc_pairs_build: active[m] != 0 keeps
+ * molecule m of the batch partition, 0 leaves its shell pairs (and so all of
+ * its quartets) out of J/K and gradient builds; NULL keeps every molecule.
+ * Drops the pair list like jqc_set_geometry.  Serves a geometry sweep whose
+ * molecules finish at different steps (geomopt/optimizer.py:130-200 per
+ * molecule). */
+int jqc_set_molecule_mask(jqc_ctx *ctx, const int *active);
+
 /* Counters of the work list for (precision_mode, mixed_tau) as jqc_jk
  * would use it: out[0] shell pairs, out[1] kept pairs, out[2] screened
  * canonical quartets on the FP64 path, out[3] on the FP32 path, out[4]
@@ -164,9 +181,11 @@ int jqc_jk(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int 
  * density-screening scratch is a static device array of 512*512 floats, so
  * contexts with more than 512 shells get JQC_ERR_TOO_LARGE.  The first call
  * on a device looks the array's address up (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the array and each
- * call rewrites it completely before reading it; calls that overlap on the
- * GPU (different streams or contexts without ordering) race on it. */
+ * first call before any stream capture.  The looked-up address belongs to
+ * the device's current primary context: after a cudaDeviceReset in the same
+ * process the entry point must not be used again.  All calls share the array
+ * and each call rewrites it completely before reading it; calls that overlap
+ * on the GPU (different streams or contexts without ordering) race on it. */
 int jqc_jk_noalloc(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K, int precision_mode,
                    double mixed_tau, double dens_tau, void *stream);
 
@@ -177,7 +196,7 @@ int jqc_jk_timed(jqc_ctx *ctx, int n_dens, const double *D, double *J, double *K
                  double mixed_tau, double dens_tau, void *stream, double *class_ms);
 
 /* CUDA graph capture of any sequence of the stream-ordered calls above
- * (jqc_jk, jqc_jk_noalloc, jqc_grad2e, jqc_grad1e, jqc_one_electron):
+ * (jqc_jk, jqc_grad2e, jqc_grad1e, jqc_one_electron):
  * jqc_graph_begin starts capturing `stream` (a created stream, not the
  * legacy default stream), the calls record their kernels instead of running
  * them, and jqc_graph_end instantiates the graph and returns its id.

@@ -70,6 +70,8 @@ SIGNATURES = {
     "jqc_class_stats": (_c_int, [_vp, _c_int, _c_dbl, _llp]),
     "jqc_fp_peak": (_c_int, [_c_int, _c_int, _c_int, _dp, _vp]),
     "jqc_batch_partition": (_c_int, [_vp, _c_int, _ip]),
+    "jqc_set_geometry": (_c_int, [_vp, _dp]),
+    "jqc_set_molecule_mask": (_c_int, [_vp, _ip]),
     "jqc_grad2e_ex": (_c_int, [_vp, _c_int, _vp, _c_dbl, _c_dbl, _c_dbl, _vp, _vp, _dp]),
     "jqc_set_grad_engine": (_c_int, [_vp, _c_int, _c_int]),
     "jqc_get_grad_engine": (_c_int, [_vp, _ip]),

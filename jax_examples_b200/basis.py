@@ -13,14 +13,15 @@ Follows the reference's basis layer:
 Basis data.  The Basis Set Exchange database is not available, so the named
 bases here are:
 
-* ``"sto-3g"`` for H and He: the STO-3G 1s parameters that the reference
-  itself carries (``fp/qchem_fp.py:64-76``).
+* ``"sto-3g"`` (H, He, C, N, O, F), ``"6-31g"``, ``"6-31g*"`` and
+  ``"6-31g**"`` (H, O): the published parameters, carried as constant tables
+  in :mod:`.basis_data` (He STO-3G is the reference's own table,
+  ``fp/qchem_fp.py:64-76``).
 * ``"syn-sto-3g"``, ``"syn-6-31g*"``, ``"syn-6-31g**"``: *synthetic* bases
   with the shell structure and contraction lengths of STO-3G / 6-31G* /
   6-31G** (Cartesian d) and exponents/coefficients generated from simple
-  closed-form sequences.  They reproduce the computational shape (shell and
-  primitive counts, angular classes, exponent spread) of the named bases,
-  not their chemistry.
+  closed-form sequences.  They exercise the kernels with other exponent
+  spreads; no workload of the benchmark uses them.
 
 Any real basis can be used by passing its BSE-schema dict to
 :func:`build_basis_set` (``basis=dict``) or by registering it with
@@ -34,6 +35,7 @@ from typing import Dict, List
 
 import numpy as np
 
+from .basis_data import real_bases
 from .core import (
     ANGSTROM_TO_BOHR,
     BasisSet,
@@ -112,12 +114,7 @@ def _bump(n: int, centre: float, width: float) -> List[float]:
     return [math.exp(-(((k - centre) / width) ** 2)) for k in range(n)]
 
 
-# STO-3G 1s for H and He as carried by the reference (fp/qchem_fp.py:64-76).
-_STO3G_1S_COEFS = [0.15432897, 0.53532814, 0.44463454]
-_STO3G = {
-    "1": {"electron_shells": [_shell(0, [3.42525091, 0.62391373, 0.16885540], _STO3G_1S_COEFS)]},
-    "2": {"electron_shells": [_shell(0, [6.36242139, 1.15892300, 0.31364979], _STO3G_1S_COEFS)]},
-}
+_STO3G = real_bases()["sto-3g"]["elements"]
 
 
 def _syn_sto3g() -> dict:
@@ -163,7 +160,7 @@ def _syn_631gs(h_p: bool) -> dict:
 
 
 _LIBRARY: Dict[str, dict] = {
-    "sto-3g": {"elements": _STO3G},
+    **real_bases(),
     "syn-sto-3g": {"elements": _syn_sto3g()},
     "syn-6-31g*": {"elements": _syn_631gs(False)},
     "syn-6-31g**": {"elements": _syn_631gs(True)},

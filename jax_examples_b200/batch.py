@@ -72,7 +72,7 @@ class MoleculeBatch:
         spherical: layout of the built bases (all bases must agree).
     """
 
-    def __init__(self, mols: Sequence, basis: str = "syn-6-31g*", bases: Optional[Sequence] = None,
+    def __init__(self, mols: Sequence, basis: str = "6-31g*", bases: Optional[Sequence] = None,
                  spherical: bool = False):
         self.mols = list(mols)
         if not self.mols:
@@ -117,6 +117,18 @@ class MoleculeBatch:
     def __len__(self) -> int:
         return len(self.mols)
 
+    def update_geometry(self, moved: dict) -> None:
+        """Replace molecule m by ``moved[m]`` (same atoms, new coordinates) for
+        every m in ``moved``; the concatenated nuclei follow.  The engine of
+        the batch is moved with :meth:`BatchedERI.update_geometry`."""
+        for m, mol in moved.items():
+            xyz = np.asarray(mol.coords, np.float64)
+            if xyz.shape != (self.n_atoms[m], 3):
+                raise ValueError(f"molecule {m}: expected {self.n_atoms[m]} atoms")
+            self.mols[m] = mol
+            o = self.atom_off[m]
+            self.coords[o:o + self.n_atoms[m]] = xyz
+
     def nuclei(self) -> _Nuclei:
         return _Nuclei(self.coords, self.atomic_numbers)
 
@@ -150,6 +162,15 @@ class BatchedERI:
     # ------------------------------------------------------------ lifecycle
     def close(self) -> None:
         self.engine.close()
+
+    def update_geometry(self, moved: dict, active: Optional[Sequence[bool]] = None) -> None:
+        """Geometry-only update of the batch (``jqc_set_geometry``): molecules
+        in ``moved`` take their new coordinates, shell pairs and Schwarz
+        bounds are rebuilt in the same context, and the launch tuning (the
+        autotuner's choice) is kept.  ``active`` (one flag per molecule)
+        leaves the other molecules out of the next builds."""
+        self.batch.update_geometry(moved)
+        self.engine.set_geometry(self.batch.coords, None if active is None else [bool(a) for a in active])
 
     @property
     def n_basis(self) -> int:
@@ -478,7 +499,8 @@ class _Group:
 
 
 def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, engine: Optional[BatchedERI] = None,
-                  use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None) -> BatchSCF:
+                  use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None,
+                  molecules: Optional[Sequence[int]] = None) -> BatchSCF:
     """Closed-shell SCF of every molecule of the batch, in lock step.
 
     Per molecule the iteration is that of ``scf/rhf.py:95-169`` (and of
@@ -491,20 +513,28 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     runs as batched tensor operations per group of equal-size molecules with
     one host read per iteration.  A converged molecule keeps its state and
     leaves the builds.
+
+    ``molecules`` restricts the SCF to those molecules of the batch (the
+    others get ``None`` results); the engine's molecule mask should leave the
+    rest out of the pair list (:meth:`BatchedERI.update_geometry`).
     """
     config = config or CalcConfig()
-    for mol in batch.mols:
+    M = len(batch)
+    sel = list(range(M)) if molecules is None else sorted({int(m) for m in molecules})
+    if not sel or sel[0] < 0 or sel[-1] >= M:
+        raise ValueError("molecules must be a non-empty subset of the batch's molecule indices")
+    for m in sel:
+        mol = batch.mols[m]
         if mol.spin != 0 or mol.n_electrons % 2 != 0:
             raise ValueError("run_rhf_batch requires closed-shell molecules (spin 0, even electron count)")
     eng = engine or BatchedERI(batch, schwarz_tau=config.schwarz_tau)
-    M = len(batch)
     t_setup = time.perf_counter()
     S_all, T_all, V_all = eng.engine.one_electron()
     H_all = T_all + V_all
     n_occ = [mol.n_electrons // 2 for mol in batch.mols]
-    E_nuc = [nuclear_repulsion_energy(mol) for mol in batch.mols]
+    E_nuc = [nuclear_repulsion_energy(mol) if m in sel else 0.0 for m, mol in enumerate(batch.mols)]
     keys = {}
-    for m in range(M):
+    for m in sel:
         keys.setdefault((batch.n_bf[m], n_occ[m]), []).append(m)
     groups = []
     for (n, no), members in keys.items():
@@ -540,7 +570,8 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
     last = torch.cat([g.E for g in groups]).cpu().numpy()
     order = [m for g in groups for m in g.members]
     pos = {m: k for k, m in enumerate(order)}
-    converged = np.zeros(M, dtype=bool)
+    converged = np.ones(M, dtype=bool)
+    converged[sel] = False
     for _ in range(config.max_scf_iter):
         if converged.all():
             break
@@ -587,7 +618,7 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
                   jk_seconds=fb.seconds(), build_ms=fb.build_ms(), setup_seconds=setup_s, graph=bool(fb.graphs),
                   autotuned=bool(autotune),
                   n_molecules=M, n_basis=batch.n_basis, precision=config.precision,
-                  incremental=fb.incremental, groups=len(groups), prepare_seconds=prepare_s,
+                  incremental=fb.incremental, groups=len(groups), prepare_seconds=prepare_s, molecules=len(sel),
                   prepare_breakdown=getattr(fb, "prep_times", {}))
     results = [None] * M
     for g in groups:
@@ -615,6 +646,8 @@ def rhf_gradient_batch(batch: MoleculeBatch, scf: BatchSCF, timing: Optional[dic
     D = torch.zeros((n, n), dtype=torch.float64, device=dev)
     W = torch.zeros_like(D)
     for m, res in enumerate(scf.results):
+        if res is None:
+            continue
         st = res.state
         batch.block(D, m).copy_(st.density)
         batch.block(W, m).copy_(energy_weighted_density(st.coefficients, st.orbital_energies,
@@ -629,6 +662,9 @@ def rhf_gradient_batch(batch: MoleculeBatch, scf: BatchSCF, timing: Optional[dic
         timing["grad_seconds"] = timing.get("grad_seconds", 0.0) + e0.elapsed_time(e1) * 1e-3
     out = []
     for m, mol in enumerate(batch.mols):
+        if scf.results[m] is None:
+            out.append(None)
+            continue
         gn = nuclear_repulsion_gradient(mol.coords, mol.atomic_numbers).to(dev)
         out.append(batch.atoms(g, m) + gn)
     return out
@@ -704,7 +740,7 @@ def _bfgs_walker(mol, max_steps: int, grad_tol: float, step_tol: float, max_step
                      n_steps=len(trajectory) - 1, trajectory=trajectory)
 
 
-def energies_and_gradients(mols: Sequence, basis: str = "syn-6-31g*", config: Optional[CalcConfig] = None,
+def energies_and_gradients(mols: Sequence, basis: str = "6-31g*", config: Optional[CalcConfig] = None,
                            use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None,
                            timing: Optional[dict] = None):
     """RHF energies and analytic gradients of many molecules in one batch:
@@ -723,35 +759,101 @@ def energies_and_gradients(mols: Sequence, basis: str = "syn-6-31g*", config: Op
     return out
 
 
-def optimize_bfgs_batch(mols: Sequence, basis: str = "syn-6-31g*", max_steps: int = 50, grad_tol: float = 1e-4,
+class _BatchEvaluator:
+    """Energies and analytic gradients of a changing subset of a fixed set of
+    molecules, on one engine that lives as long as the evaluator.
+
+    The first call builds the context (and, with ``autotune``, tunes the
+    launches); every later call moves the nuclei in place
+    (:meth:`BatchedERI.update_geometry`), rebuilds only the shell pairs and
+    work lists, leaves the molecules not asked for out of the pair list, and
+    keeps the tuning.  Each evaluation is a full SCF from the core guess, as
+    ``_energy_and_gradient`` (``geomopt/optimizer.py:55-76``) does."""
+
+    def __init__(self, mols: Sequence, basis: str, config: CalcConfig, use_graph: bool = True,
+                 autotune: bool = False, tune_cache: Optional[str] = None, timing: Optional[dict] = None):
+        self.mols = list(mols)
+        self.batch = MoleculeBatch(self.mols, basis)
+        self.config, self.use_graph, self.autotune, self.tune_cache = config, use_graph, autotune, tune_cache
+        self.timing = timing
+        self.gtau = MIXED_GRAD_TAU if config.precision == "mixed" else 0.0
+        self.eng = None
+        self.rounds = 0
+
+    def __call__(self, coords: dict) -> dict:
+        """{i: (energy, gradient (n_atoms, 3) ndarray)} for {i: coords}."""
+        ids = sorted(coords)
+        mols = self.mols
+        moved = {i: make_molecule(mols[i].elements, coords[i], np.asarray(mols[i].atomic_numbers),
+                                  charge=mols[i].charge, spin=mols[i].spin) for i in ids}
+        t0 = time.perf_counter()
+        mask = [m in moved for m in range(len(mols))]
+        if self.eng is None:
+            self.eng = BatchedERI(self.batch, schwarz_tau=self.config.schwarz_tau)
+            same = all(np.array_equal(np.asarray(moved[i].coords, np.float64),
+                                      np.asarray(mols[i].coords, np.float64)) for i in ids)
+            if not (same and all(mask)):
+                self.eng.update_geometry(moved, mask)
+        else:
+            self.eng.update_geometry(moved, mask)
+        t_geom = time.perf_counter() - t0
+        scf = run_rhf_batch(self.batch, self.config, engine=self.eng, use_graph=self.use_graph,
+                            autotune=self.autotune and self.rounds == 0, tune_cache=self.tune_cache, molecules=ids)
+        grads = rhf_gradient_batch(self.batch, scf, self.timing, self.gtau)
+        tm = self.timing
+        if tm is not None:
+            rec = scf.record
+            tm["jk_seconds"] = tm.get("jk_seconds", 0.0) + rec["jk_seconds"]
+            tm["fock_builds"] = tm.get("fock_builds", 0) + rec["fock_builds"]
+            tm["evaluations"] = tm.get("evaluations", 0) + len(ids)
+            tm["batches"] = tm.get("batches", 0) + 1
+            tm["geometry_update_seconds"] = tm.get("geometry_update_seconds", 0.0) + t_geom
+            tm["setup_seconds"] = tm.get("setup_seconds", 0.0) + rec["setup_seconds"]
+            br = tm.setdefault("prepare_breakdown", {})
+            for k, v in rec.get("prepare_breakdown", {}).items():
+                br[k] = br.get(k, 0.0) + v
+        self.rounds += 1
+        return {i: (scf.results[i].energy, grads[i].cpu().numpy()) for i in ids}
+
+    def close(self) -> None:
+        if self.eng is not None:
+            self.eng.close()
+            self.eng = None
+
+
+def optimize_bfgs_batch(mols: Sequence, basis: str = "6-31g*", max_steps: int = 50, grad_tol: float = 1e-4,
                         step_tol: float = 1e-6, scf_conv: float = 1e-10, max_step_size: float = 0.3,
                         config: Optional[CalcConfig] = None, use_graph: bool = True, autotune: bool = False,
                         tune_cache: Optional[str] = None, timing: Optional[dict] = None) -> List[OptResult]:
     """BFGS geometry optimisation of every molecule (``optimize_bfgs`` of
     ``geomopt/optimizer.py:79-209`` per molecule, RHF).  Every round collects
     the geometry each unfinished optimisation needs next (a step or a
-    line-search trial) and evaluates all of them in one batch."""
+    line-search trial) and evaluates all of them in one batch, on one engine
+    kept for the whole optimisation (geometry-only updates between rounds,
+    tuning done once: :class:`_BatchEvaluator`)."""
     config = config or CalcConfig(scf_conv=scf_conv, max_scf_iter=200)
     walkers = [_bfgs_walker(m, max_steps, grad_tol, step_tol, max_step_size) for m in mols]
     pending = {i: w.send(None) for i, w in enumerate(walkers)}
     results: List[Optional[OptResult]] = [None] * len(mols)
-    while pending:
-        ids = sorted(pending)
-        geoms = [make_molecule(mols[i].elements, pending[i], np.asarray(mols[i].atomic_numbers),
-                               charge=mols[i].charge, spin=mols[i].spin) for i in ids]
-        evals = energies_and_gradients(geoms, basis, config, use_graph=use_graph, autotune=autotune,
-                                       tune_cache=tune_cache, timing=timing)
-        nxt = {}
-        for i, (e, g, _res) in zip(ids, evals):
-            try:
-                nxt[i] = walkers[i].send((e, g))
-            except StopIteration as stop:
-                results[i] = stop.value
-        pending = nxt
+    ev = _BatchEvaluator(mols, basis, config, use_graph, autotune, tune_cache, timing)
+    try:
+        while pending:
+            out = ev(pending)
+            nxt = {}
+            for i in sorted(pending):
+                try:
+                    nxt[i] = walkers[i].send(out[i])
+                except StopIteration as stop:
+                    results[i] = stop.value
+            pending = nxt
+    finally:
+        ev.close()
+    if timing is not None:
+        timing["rounds"] = ev.rounds
     return results
 
 
-def optimize_bfgs(mol, basis_name: str = "syn-6-31g*", method: str = "rhf", max_steps: int = 50,
+def optimize_bfgs(mol, basis_name: str = "6-31g*", method: str = "rhf", max_steps: int = 50,
                   grad_tol: float = 1e-4, step_tol: float = 1e-6, scf_conv: float = 1e-10,
                   max_step_size: float = 0.3, verbose: int = 0) -> OptResult:
     """Single-molecule ``optimize_bfgs`` (``geomopt/optimizer.py:79-209``)

@@ -249,6 +249,7 @@ struct jqc_ctx {
   // batch partition: molecule of each shell / atom (one molecule by default)
   int n_mol = 1;
   std::vector<int> shell_mol, atom_mol;
+  std::vector<int> mol_active;  // empty: every molecule takes part in the pair list
   DevBuf<int> d_shell_mol, d_atom_mol;
   // pairs (sorted: block by (class, K_a, K_b), Q descending inside)
   bool pairs_ready = false;
@@ -785,6 +786,7 @@ int jqc_basis_upload(jqc_ctx* c, int n_shell, const int* l, const int* nprim, co
   c->n_mol = 1;
   c->shell_mol.assign(n_shell, 0);
   c->atom_mol.assign(n_atom, 0);
+  c->mol_active.clear();
   JQC_CUDA_CHECK(cudaStreamSynchronize(s0));
   c->basis_ready = true;
   c->pairs_ready = false;
@@ -806,12 +808,52 @@ int jqc_batch_partition(jqc_ctx* c, int n_mol, const int* mol_of_atom) {
   int rc = select_device(c);
   if (rc) return rc;
   c->n_mol = n_mol;
+  c->mol_active.clear();
   c->atom_mol.assign(mol_of_atom, mol_of_atom + c->n_atom);
   for (int s = 0; s < c->n_shell; ++s) c->shell_mol[s] = c->atom_mol[c->atom[s]];
   cudaStream_t s0 = 0;
   JQC_CUDA_CHECK(c->d_shell_mol.upload(c->shell_mol, s0));
   JQC_CUDA_CHECK(c->d_atom_mol.upload(c->atom_mol, s0));
   JQC_CUDA_CHECK(cudaStreamSynchronize(s0));
+  c->pairs_ready = false;
+  drop_jk_tasks(c);
+  c->full_tasks.valid = false;
+  c->grad_tasks.valid = false;
+  return JQC_OK;
+}
+
+int jqc_set_geometry(jqc_ctx* c, const double* atom_xyz) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_set_geometry: null context");
+  JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_set_geometry: call jqc_basis_upload first");
+  JQC_REQUIRE(c->n_atom > 0, JQC_ERR_NOT_READY, "jqc_set_geometry: the basis was uploaded without atoms");
+  JQC_REQUIRE(atom_xyz != nullptr, JQC_ERR_INVALID, "jqc_set_geometry: null atom_xyz");
+  for (int i = 0; i < 3 * c->n_atom; ++i)
+    JQC_REQUIRE(std::isfinite(atom_xyz[i]), JQC_ERR_INVALID, "jqc_set_geometry: non-finite coordinate");
+  int rc = select_device(c);
+  if (rc) return rc;
+  c->atom_xyz.assign(atom_xyz, atom_xyz + 3 * c->n_atom);
+  for (int s = 0; s < c->n_shell; ++s)
+    for (int k = 0; k < 3; ++k) c->centres[3 * s + k] = atom_xyz[3 * c->atom[s] + k];
+  cudaStream_t s0 = 0;
+  JQC_CUDA_CHECK(c->d_centres.upload(c->centres, s0));
+  JQC_CUDA_CHECK(c->d_atom_xyz.upload(c->atom_xyz, s0));
+  JQC_CUDA_CHECK(cudaStreamSynchronize(s0));
+  c->pairs_ready = false;
+  drop_jk_tasks(c);
+  c->full_tasks.valid = false;
+  c->grad_tasks.valid = false;
+  return JQC_OK;
+}
+
+int jqc_set_molecule_mask(jqc_ctx* c, const int* active) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_set_molecule_mask: null context");
+  JQC_REQUIRE(c->basis_ready, JQC_ERR_NOT_READY, "jqc_set_molecule_mask: call jqc_basis_upload first");
+  if (active == nullptr) {
+    c->mol_active.clear();
+  } else {
+    c->mol_active.assign(active, active + c->n_mol);
+    for (int& a : c->mol_active) a = a != 0;
+  }
   c->pairs_ready = false;
   drop_jk_tasks(c);
   c->full_tasks.valid = false;
@@ -836,6 +878,7 @@ int jqc_pairs_build(jqc_ctx* c, double schwarz_tau, double prim_tau, void* strea
   for (int i = 0; i < c->n_shell; ++i)
     for (int j = 0; j <= i; ++j) {
       if (c->shell_mol[i] != c->shell_mol[j]) continue;  // no pairs across molecules
+      if (!c->mol_active.empty() && !c->mol_active[c->shell_mol[i]]) continue;  // molecule left out
       int a = i, b = j;
       if (c->l[a] < c->l[b]) std::swap(a, b);
       ShellPair sp;

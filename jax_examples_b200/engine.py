@@ -107,6 +107,7 @@ class DirectERI:
         self.basis = basis
         self.packed = pk = PackedBasis(basis)
         self.schwarz_tau = float(schwarz_tau)
+        self.prim_tau = float(prim_tau)
         if mol is not None:
             self.atom_xyz = np.ascontiguousarray(np.asarray(mol.coords, np.float64))
             self.atom_Z = np.ascontiguousarray(np.asarray(mol.atomic_numbers, np.float64))
@@ -143,6 +144,30 @@ class DirectERI:
                 r += m.shape[0]
                 c += m.shape[1]
             self._C = torch.tensor(C, dtype=torch.float64, device=self.device)
+
+    # ------------------------------------------------------------ geometry
+    def set_geometry(self, coords, active=None) -> None:
+        """Move the nuclei (and every shell with its atom) to ``coords``
+        (n_atom, 3) bohr and rebuild the shell pairs, keeping the basis, the
+        batch partition and the launch tuning (``jqc_set_geometry`` +
+        ``jqc_pairs_build``).  ``active`` (one flag per molecule of the batch
+        partition) leaves the pairs of inactive molecules out of the builds."""
+        xyz = np.ascontiguousarray(np.asarray(coords, dtype=np.float64))
+        if xyz.shape != self.atom_xyz.shape:
+            raise ValueError(f"coords must have shape {self.atom_xyz.shape}; got {xyz.shape}")
+        dp = lambda a: a.ctypes.data_as(_abi._dp)  # noqa: E731
+        with torch.cuda.device(self.device):
+            _abi.call("jqc_set_geometry", self._ctx, dp(xyz))
+            if active is not None:
+                act = np.ascontiguousarray(np.asarray(active, dtype=np.int32))
+                if act.shape != (self.n_mol,):
+                    raise ValueError(f"active must have one flag per molecule ({self.n_mol})")
+                _abi.call("jqc_set_molecule_mask", self._ctx, act.ctypes.data_as(_abi._ip))
+            else:
+                _abi.call("jqc_set_molecule_mask", self._ctx, None)
+            _abi.call("jqc_pairs_build", self._ctx, self.schwarz_tau, float(self.prim_tau), _stream(self.device))
+        self.atom_xyz = xyz
+        self.packed.centres = np.ascontiguousarray(xyz[self.packed.atom])
 
     # ------------------------------------------------------------ lifecycle
     def close(self) -> None:

@@ -225,6 +225,51 @@ def nuclear_repulsion(coords, Z) -> float:
     return total
 
 
+# ---------------------------------------------------------------- spherical
+
+
+def cart_to_spherical(l: int) -> np.ndarray:
+    """(2l+1, ncart) map of ``integrals/spherical.py:34-67``: identity for
+    s and p; for d the real solid harmonics in libcint row order
+    (xy, yz, z^2, xz, x^2-y^2) over the Cartesian columns xx, xy, xz, yy,
+    yz, zz, all components sharing one normalization."""
+    if l == 0:
+        return np.ones((1, 1))
+    if l == 1:
+        return np.eye(3)
+    if l == 2:
+        m = np.zeros((5, 6))
+        r3 = np.sqrt(3.0)
+        m[0, 1] = r3
+        m[1, 4] = r3
+        m[2, [0, 3, 5]] = (-0.5, -0.5, 1.0)
+        m[3, 2] = r3
+        m[4, [0, 3]] = (r3 / 2.0, -r3 / 2.0)
+        return m
+    raise NotImplementedError(f"Cart-to-spherical transformation only implemented for l <= 2 (got l={l}).")
+
+
+def spherical_matrix(basis) -> np.ndarray:
+    """Block-diagonal C (n_sph, n_cart) over the shells in basis order, so
+    that M_sph = C M_cart C^T (``eri.py:61-66,100-103`` per block)."""
+    blocks = [cart_to_spherical(int(s.angular_momentum)) for s in basis.shells]
+    C = np.zeros((sum(b.shape[0] for b in blocks), sum(b.shape[1] for b in blocks)))
+    r = c = 0
+    for b in blocks:
+        C[r:r + b.shape[0], c:c + b.shape[1]] = b
+        r += b.shape[0]
+        c += b.shape[1]
+    return C
+
+
+def eri_to_spherical(eri, C) -> np.ndarray:
+    """(pq|rs) = sum C_pi C_qj C_rk C_sl (ij|kl), one index at a time."""
+    t = np.tensordot(C, eri, axes=(1, 0))
+    t = np.tensordot(C, t, axes=(1, 1)).transpose(1, 0, 2, 3)
+    t = np.tensordot(t, C, axes=(2, 1)).transpose(0, 1, 3, 2)
+    return np.tensordot(t, C, axes=(3, 1))
+
+
 # ---------------------------------------------------------------- SCF / DIIS
 
 
@@ -373,11 +418,17 @@ def uhf(S, H, jk: Callable, n_alpha: int, n_beta: int, conv: float = 1e-10, max_
 # ------------------------------------------------------------ gradients
 
 
-def rhf_energy(mol, build_basis: Callable, mode: int = 1, conv: float = 1e-10):
-    """Total RHF energy through the oracle (dense tensor; small systems)."""
+def rhf_energy(mol, build_basis: Callable, mode: int = 1, conv: float = 1e-10, spherical: bool = False):
+    """Total RHF energy through the oracle (dense tensor; small systems).
+    ``spherical`` runs the SCF in the solid-harmonic basis of the shells, as
+    the reference does for ``BasisSet.spherical``."""
     basis = build_basis(mol)
     S, T, V = one_electron(basis, mol, mode)
     eri = eri_tensor(basis, mode)
+    if spherical:
+        C = spherical_matrix(basis)
+        S, T, V = (C @ M @ C.T for M in (S, T, V))
+        eri = eri_to_spherical(eri, C)
     E, D, C, eps, F, it, ok = rhf(S, T + V, lambda D: jk_from_tensor(D, eri), mol.n_electrons // 2, conv=conv)
     return E + nuclear_repulsion(mol.coords, mol.atomic_numbers), D, C, eps, ok
 

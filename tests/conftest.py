@@ -39,7 +39,7 @@ class Golden:
     def basis(self):
         from jax_examples_b200.basis import build_basis_set
 
-        return build_basis_set(self.molecule(), self.rec["basis"])
+        return build_basis_set(self.molecule(), self.rec["basis"], spherical=bool(self.rec.get("spherical", False)))
 
 
 @pytest.fixture(scope="session")

@@ -101,4 +101,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("JQC_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: gen_bfgs_golden.py REFERENCE_ROOT (or set JQC_REFERENCE_ROOT)")
+    main(root)

@@ -65,13 +65,30 @@ def test_water_cluster_shapes():
     for n, nbf, nbf2 in ((1, 19, 25), (8, 152, 200), (16, 304, 400)):
         mol = pb.water_cluster(n, seed=0)
         assert mol.n_electrons == 10 * n
-        assert pb.build_basis_set(mol, "syn-6-31g*").n_basis == nbf
-        assert pb.build_basis_set(mol, "syn-6-31g**").n_basis == nbf2
+        for prefix in ("", "syn-"):
+            assert pb.build_basis_set(mol, prefix + "6-31g*").n_basis == nbf
+            assert pb.build_basis_set(mol, prefix + "6-31g**").n_basis == nbf2
     # lattice spacing 2.9 A between O atoms
     mol = pb.water_cluster(8, seed=3)
     O = mol.coords[0::3]
     d = np.linalg.norm(O[1] - O[0]) * 0.529177210903
     assert abs(d - 2.9) < 1e-12
+
+
+def test_published_basis_shapes():
+    """Shell structure of the published bases for water: 18 spherical
+    functions in 6-31G* (the reference's tests/test_basis.py:191-206), 7 in
+    STO-3G; contraction lengths of 6-31G (O 1s has six primitives)."""
+    mol = pb.water_cluster(1)
+    assert pb.build_basis_set(mol, "6-31g*", spherical=True).n_basis == 18
+    assert pb.build_basis_set(mol, "6-31g**", spherical=True).n_basis == 24
+    bs = pb.build_basis_set(mol, "sto-3g")
+    assert bs.n_basis == 7 and [s.angular_momentum for s in bs.shells] == [0, 0, 1, 0, 0]
+    bs = pb.build_basis_set(mol, "6-31g*")
+    o = [(s.angular_momentum, len(s.exponents)) for s in bs.shells if s.atom_index == 0]
+    assert o == [(0, 6), (0, 3), (0, 1), (1, 3), (1, 1), (2, 1)]
+    h = [(s.angular_momentum, len(s.exponents)) for s in pb.build_basis_set(mol, "6-31g**").shells if s.atom_index == 1]
+    assert h == [(0, 3), (0, 1), (1, 1)]
 
 
 def test_basis_errors_mirror_reference():

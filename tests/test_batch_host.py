@@ -64,15 +64,23 @@ def test_batched_bfgs_rounds_equal_independent_runs(monkeypatch):
     by_natoms = {len(m.atomic_numbers): np.array(r["r0"]) for m, r in zip(mols, recs)}
     calls = []
 
-    def fake(geoms, basis, config, **kw):
-        calls.append(len(geoms))
-        out = []
-        for g in geoms:
-            e, gr = model_energy_gradient(np.asarray(g.coords), by_natoms[len(g.atomic_numbers)])
-            out.append((e, gr, None))
-        return out
+    class FakeEvaluator:
+        """Stands in for the device evaluator: the model potential per molecule."""
 
-    monkeypatch.setattr(jb, "energies_and_gradients", fake)
+        def __init__(self, mols_, basis, config, *a):
+            self.mols = mols_
+            self.rounds = 0
+
+        def __call__(self, coords):
+            calls.append(len(coords))
+            self.rounds += 1
+            return {i: model_energy_gradient(np.asarray(c), by_natoms[len(self.mols[i].atomic_numbers)])
+                    for i, c in coords.items()}
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(jb, "_BatchEvaluator", FakeEvaluator)
     res = jb.optimize_bfgs_batch(mols, "model", max_steps=25, grad_tol=1e-5)
     for m, rec in zip(res, recs):
         assert m.n_steps == rec["n_steps"] and m.converged == rec["converged"]
@@ -84,7 +92,7 @@ def test_batched_bfgs_rounds_equal_independent_runs(monkeypatch):
 
 def test_molecule_batch_layout():
     mols = [pb.water_cluster(n, seed=n) for n in (2, 1, 3)]
-    b = jb.MoleculeBatch(mols, "syn-6-31g*")
+    b = jb.MoleculeBatch(mols, "6-31g*")
     assert b.n_bf == [38, 19, 57] and b.bf_off == [0, 38, 57] and b.n_basis == 114
     assert b.atom_off == [0, 6, 9] and b.n_atoms == [6, 3, 9]
     np.testing.assert_array_equal(b.mol_of_atom, [0] * 6 + [1] * 3 + [2] * 9)
@@ -102,4 +110,4 @@ def test_molecule_batch_layout():
     blk = b.block(torch.tensor(M), 1)
     np.testing.assert_array_equal(blk.numpy(), M[38:57, 38:57])
     with pytest.raises(ValueError):
-        jb.MoleculeBatch([], "syn-6-31g*")
+        jb.MoleculeBatch([], "6-31g*")

@@ -18,8 +18,23 @@ import torch
 import oracle
 from conftest import GOLDEN, ROOT
 
-REF = os.environ.get("JQC_REFERENCE_ROOT", "/root/reference")
-pytestmark = pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "jax_qc")), reason="reference not available")
+def _reference_root() -> str:
+    """The reference checkout: ``JQC_REFERENCE_ROOT``, else the parent of an
+    importable ``jax_qc`` package; empty when neither exists."""
+    root = os.environ.get("JQC_REFERENCE_ROOT", "")
+    if root:
+        return root
+    import importlib.util
+
+    spec = importlib.util.find_spec("jax_qc") if "jax_qc" not in sys.modules else None
+    if spec is not None and spec.origin:
+        return os.path.dirname(os.path.dirname(spec.origin))
+    return ""
+
+
+REF = _reference_root()
+pytestmark = pytest.mark.skipif(not REF or not os.path.isdir(os.path.join(REF, "jax_qc")),
+                                reason="reference checkout not available (set JQC_REFERENCE_ROOT)")
 
 
 class FakeDirect:

@@ -22,7 +22,7 @@ from jax_examples_b200.grad import rhf_gradient
 pytestmark = pytest.mark.gpu
 
 DEV = "cuda:0"
-BASIS = "syn-6-31g*"
+BASIS = "6-31g*"
 
 
 def _mols(sizes, seed=0, noise=0.05):
@@ -64,7 +64,7 @@ def test_batch_jk_matches_each_molecule_alone():
 
 def test_batch_jk_vs_oracle_small():
     mols = [pb.water_cluster(1, seed=1, noise_angstrom=0.05), pb.water_cluster(1, seed=2, noise_angstrom=0.05)]
-    batch = MoleculeBatch(mols, "syn-sto-3g")
+    batch = MoleculeBatch(mols, "sto-3g")
     eng = BatchedERI(batch, schwarz_tau=0.0)
     rng = np.random.default_rng(5)
     Dn = _random_block_density(batch, rng)
@@ -262,6 +262,53 @@ def test_bfgs_batch_matches_single_molecule_runs():
         e_a = np.array([e for _, e in alone.trajectory])
         np.testing.assert_allclose(e_b, e_a, atol=1e-8, rtol=0)
         assert np.all(np.diff(e_b) <= 1e-10)  # Armijo steps never raise the energy
+
+
+def test_geometry_update_and_molecule_mask_match_fresh_engines():
+    """jqc_set_geometry + jqc_molecule_mask in one context give the J/K,
+    one-electron integrals and gradient of fresh engines at the new geometry
+    (1e-10); masked molecules contribute nothing; the launch tuning
+    survives the update."""
+    from jax_examples_b200.grad import grad_two_electron
+
+    mols = _mols([2, 1, 3], seed=41, noise=0.05)
+    batch = MoleculeBatch(mols, BASIS)
+    eng = BatchedERI(batch, schwarz_tau=1e-12)
+    tuned = eng.tuning().copy()
+    tuned[0, 0] = 64 if tuned[0, 0] != 64 else 256
+    eng.set_tuning(tuned)
+    rng = np.random.default_rng(42)
+    moved = {}
+    for m in range(3):  # small displacements, as a BFGS step makes
+        xyz = np.asarray(mols[m].coords) + rng.normal(0.0, 0.05, np.asarray(mols[m].coords).shape)
+        moved[m] = pb.make_molecule(mols[m].elements, xyz, mols[m].atomic_numbers)
+    eng.update_geometry({0: moved[0], 2: moved[2]}, [True, False, True])
+    np.testing.assert_array_equal(eng.tuning(), tuned)
+    D = torch.tensor(_random_block_density(batch, rng), device=DEV)[None].contiguous()
+    J, K = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J, K)
+    S, T, V = eng.engine.one_electron()
+    g2 = grad_two_electron(eng.engine, [D[0]], 1.0, 0.5)
+    for m in range(3):
+        o, k = batch.bf_off[m], batch.n_bf[m]
+        blk = (slice(o, o + k), slice(o, o + k))
+        if m == 1:  # left out: no quartets, no forces
+            assert float(J[0][blk].abs().max()) == 0.0 and float(K[0][blk].abs().max()) == 0.0
+            assert float(batch.atoms(g2, m).abs().max()) == 0.0
+            continue
+        mol = moved[m]
+        np.testing.assert_allclose(np.asarray(batch.mols[m].coords), np.asarray(mol.coords), atol=0)
+        single = DirectERI(pb.build_basis_set(mol, BASIS), mol, device=0, schwarz_tau=1e-12)
+        Js, Ks = single.jk(D[0][blk].contiguous())
+        np.testing.assert_allclose(J[0][blk].cpu().numpy(), Js.cpu().numpy(), atol=1e-10, rtol=0)
+        np.testing.assert_allclose(K[0][blk].cpu().numpy(), Ks.cpu().numpy(), atol=1e-10, rtol=0)
+        Ss, Ts, Vs = single.one_electron()
+        np.testing.assert_allclose(S[blk].cpu().numpy(), Ss.cpu().numpy(), atol=1e-12, rtol=0)
+        np.testing.assert_allclose(V[blk].cpu().numpy(), Vs.cpu().numpy(), atol=1e-11, rtol=0)
+        gs = grad_two_electron(single, [D[0][blk].contiguous()], 1.0, 0.5)
+        np.testing.assert_allclose(batch.atoms(g2, m).cpu().numpy(), gs.cpu().numpy(), atol=1e-10, rtol=0)
+        single.close()
+    eng.close()
 
 
 def _set_grad_engines(eng, engine, classes):

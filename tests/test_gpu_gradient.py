@@ -22,8 +22,11 @@ def _scf(mol, bs, **kw):
     return run_scf(mol, ints, CalcConfig(method="uhf" if mol.spin else "rhf", scf_conv=1e-11, **kw))
 
 
-def test_rhf_gradient_vs_reference_golden(golden):
-    g = golden("water_synsto3g")
+@pytest.mark.parametrize("tag", ["water_synsto3g", "water_sto3g"])
+def test_rhf_gradient_vs_reference_golden(golden, tag):
+    """The reference's own gradient (central FD of its integrals,
+    rhf_grad.py:106-211) of the STO-3G water: config 1's molecule."""
+    g = golden(tag)
     mol, bs = g.molecule(), g.basis()
     res = _scf(mol, bs)
     grad = rhf_gradient(mol, res).cpu().numpy()
@@ -34,7 +37,7 @@ def test_rhf_gradient_vs_reference_golden(golden):
 
 def test_rhf_gradient_d_shells_vs_oracle_fd():
     mol = pb.water_cluster(1)
-    build = lambda m: pb.build_basis_set(m, "syn-6-31g*")  # noqa: E731
+    build = lambda m: pb.build_basis_set(m, "6-31g*")  # noqa: E731
     bs = build(mol)
     res = _scf(mol, bs)
     grad = rhf_gradient(mol, res).cpu().numpy()
@@ -46,7 +49,7 @@ def test_rhf_gradient_d_shells_vs_oracle_fd():
 
 def test_autograd_matches_direct():
     mol = pb.water_cluster(2, seed=4)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     res = _scf(mol, bs, tau=1e-13)
     g1 = rhf_gradient(mol, res).cpu().numpy()
     g2 = rhf_gradient(mol, res, autograd=True).cpu().numpy()
@@ -55,7 +58,7 @@ def test_autograd_matches_direct():
 
 def test_rhf_gradient_vs_energy_fd_dimer():
     mol = pb.water_cluster(2, seed=2)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     res = _scf(mol, bs, tau=1e-14)
     grad = rhf_gradient(mol, res).cpu().numpy()
     rng = np.random.default_rng(0)
@@ -67,16 +70,17 @@ def test_rhf_gradient_vs_energy_fd_dimer():
             c = np.array(mol.coords, dtype=float)
             c[a, k] += sgn * h
             m = make_molecule(mol.elements, c, mol.atomic_numbers)
-            e.append(_scf(m, pb.build_basis_set(m, "syn-6-31g*"), tau=1e-14).energy)
+            e.append(_scf(m, pb.build_basis_set(m, "6-31g*"), tau=1e-14).energy)
         assert abs((e[0] - e[1]) / (2 * h) - grad[a, k]) < 2e-6
 
 
-def test_uhf_gradient_vs_numerical(golden):
-    g = golden("water_cation_synsto3g_uhf")
+@pytest.mark.parametrize("tag", ["water_cation_synsto3g_uhf", "water_cation_sto3g_uhf"])
+def test_uhf_gradient_vs_numerical(golden, tag):
+    g = golden(tag)
     mol, bs = g.molecule(), g.basis()
     res = _scf(mol, bs)
     grad = uhf_gradient(mol, res).cpu().numpy()
-    num = numerical_gradient(mol, "syn-sto-3g", step_size=1e-4, scf_conv=1e-11, device=0).numpy()
+    num = numerical_gradient(mol, g.rec["basis"], step_size=1e-4, scf_conv=1e-11, device=0).numpy()
     np.testing.assert_allclose(grad, num, atol=2e-6)
 
 
@@ -86,10 +90,10 @@ def test_drop_in_gradient_entry_point():
     from jax_examples_b200 import drop_in
 
     mol = pb.water_cluster(2, seed=3)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     ints = compute_integrals(mol, bs, device=0)
     res = run_scf(mol, ints, CalcConfig(scf_conv=1e-10))
-    g = drop_in.rhf_gradient(mol, res, basis_name="syn-6-31g*", step_size=1e-4)
+    g = drop_in.rhf_gradient(mol, res, basis_name="6-31g*", step_size=1e-4)
     ref = rhf_gradient(mol, res, bs).cpu().numpy()
     assert isinstance(g, np.ndarray) and g.shape == (6, 3)
     np.testing.assert_allclose(g, ref, atol=1e-12, rtol=0)
@@ -97,13 +101,13 @@ def test_drop_in_gradient_entry_point():
 
 
 def test_h2o16_gradient_vs_central_fd_six_coordinates():
-    """The (H2O)16 6-31G*-shaped workload: analytic gradient against finite
+    """The (H2O)16 6-31G* workload: analytic gradient against finite
     differences of SCF energies (h = 1e-4 bohr, the fourth-order central
     stencil: the forces of this unrelaxed lattice reach 0.5 Eh/bohr, where
     the two-point stencil's h^2 error is ~3e-6) at 6 seeded coordinates; SCF
     converged to 1e-11 so the FD noise stays near 2e-7."""
     mol = pb.water_cluster(16, seed=0)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     cfg = CalcConfig(scf_conv=1e-11, schwarz_tau=1e-13, incremental=False)  # full FP64 builds: smooth E(R)
     ints = compute_integrals(mol, bs, device=0, schwarz_tau=1e-13)
     res = run_scf(mol, ints, cfg)
@@ -117,7 +121,7 @@ def test_h2o16_gradient_vs_central_fd_six_coordinates():
             xyz = np.array(mol.coords, dtype=np.float64)
             xyz[a, x] += k * h
             m2 = make_molecule(mol.elements, xyz, np.asarray(mol.atomic_numbers))
-            b2 = pb.build_basis_set(m2, "syn-6-31g*")
+            b2 = pb.build_basis_set(m2, "6-31g*")
             e[k] = run_scf(m2, compute_integrals(m2, b2, device=0, schwarz_tau=1e-13), cfg).energy
         fd = (8.0 * (e[1] - e[-1]) - (e[2] - e[-2])) / (12.0 * h)
         assert abs(fd - g[a, x]) < 1e-6, (a, x, fd, g[a, x])

@@ -88,8 +88,11 @@ def test_primitive_blocks_vs_golden():
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-10 * max(1.0, np.abs(ref).max()))
 
 
-def test_eri_tensor_water_synsto3g_vs_golden(golden):
-    g = golden("water_synsto3g")
+@pytest.mark.parametrize("tag", ["water_synsto3g", "water_sto3g"])
+def test_eri_tensor_water_sto3g_vs_golden(golden, tag):
+    """Full 7^4 tensor of the STO-3G water (the reference's config-1 oracle
+    case) against the reference's own tensor, and its 8-fold symmetry."""
+    g = golden(tag)
     eng = DirectERI(g.basis(), g.molecule(), device=0, schwarz_tau=0.0)
     eri = eng.eri_tensor().cpu().numpy()
     np.testing.assert_allclose(eri, g.arr["eri"], atol=1e-10, rtol=0)
@@ -98,8 +101,9 @@ def test_eri_tensor_water_synsto3g_vs_golden(golden):
     np.testing.assert_allclose(eri, eri.transpose(2, 3, 0, 1), atol=0)
 
 
-def test_eri_tensor_water_syn631gs_vs_golden(golden):
-    g = golden("water_syn631gs")
+@pytest.mark.parametrize("tag", ["water_syn631gs", "water_631gs"])
+def test_eri_tensor_water_631gs_vs_golden(golden, tag):
+    g = golden(tag)
     eng = DirectERI(g.basis(), g.molecule(), device=0, schwarz_tau=0.0)
     eri = eng.eri_tensor().cpu().numpy()
     i = g.arr["eri_idx"]
@@ -108,7 +112,10 @@ def test_eri_tensor_water_syn631gs_vs_golden(golden):
     np.testing.assert_allclose(eri, ref, atol=1e-10, rtol=0)
 
 
-@pytest.mark.parametrize("tag", ["water_synsto3g", "water_syn631gs"])
+REAL_AND_SYN = ["water_synsto3g", "water_syn631gs", "water_sto3g", "water_631gs", "water_631gss_sph"]
+
+
+@pytest.mark.parametrize("tag", REAL_AND_SYN)
 def test_one_electron_and_schwarz_vs_golden(golden, tag):
     g = golden(tag)
     eng = DirectERI(g.basis(), g.molecule(), device=0, schwarz_tau=0.0)
@@ -119,7 +126,7 @@ def test_one_electron_and_schwarz_vs_golden(golden, tag):
     np.testing.assert_allclose(eng.schwarz().cpu().numpy(), g.arr["Q"], atol=1e-12)
 
 
-@pytest.mark.parametrize("tag", ["water_synsto3g", "water_syn631gs"])
+@pytest.mark.parametrize("tag", REAL_AND_SYN)
 def test_jk_rhf_uhf_vs_golden(golden, tag):
     g = golden(tag)
     eng = DirectERI(g.basis(), g.molecule(), device=0, schwarz_tau=0.0)
@@ -135,7 +142,7 @@ def test_jk_rhf_uhf_vs_golden(golden, tag):
 
 def test_jk_cluster_vs_oracle_direct():
     mol = pb.water_cluster(3, seed=1)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     rng = np.random.default_rng(3)
     n = bs.n_basis
     D = rng.standard_normal((n, n)) * 0.05
@@ -158,7 +165,20 @@ def test_jk_cluster_vs_oracle_direct():
     assert np.max(np.abs(K3.cpu().numpy() - Kr)) < 1e-7
 
 
-@pytest.mark.parametrize("tag", ["water_synsto3g", "water_syn631gs", "water_cation_synsto3g_uhf"])
+def test_eri_tensor_spherical_vs_golden(golden):
+    """6-31G** water in the solid-harmonic basis (the reference default):
+    the tensor through the engine's spherical map against the reference's
+    ``_spherical_eri_block`` values (``eri.py:61-66,100-103``)."""
+    g = golden("water_631gss_sph")
+    eng = DirectERI(g.basis(), g.molecule(), device=0, schwarz_tau=0.0)
+    eri = eng.eri_tensor().cpu().numpy()
+    assert eri.shape == (24,) * 4
+    i = g.arr["eri_idx"]
+    np.testing.assert_allclose(eri[i[:, 0], i[:, 1], i[:, 2], i[:, 3]], g.arr["eri_val"], atol=1e-10, rtol=0)
+
+
+@pytest.mark.parametrize("tag", ["water_synsto3g", "water_syn631gs", "water_cation_synsto3g_uhf",
+                                 "water_sto3g", "water_cation_sto3g_uhf", "water_631gs", "water_631gss_sph"])
 def test_scf_energy_vs_golden(golden, tag):
     g = golden(tag)
     mol, bs = g.molecule(), g.basis()
@@ -178,3 +198,22 @@ def test_tier1_golden_energies_gpu():
         res = run_scf(mol, ints, CalcConfig(scf_conv=1e-10))
         assert abs(res.energy - d["reference_energy"]) < 1e-8, name
         assert abs(res.energy - d["golden_pyscf"]) < 1e-6, name
+
+
+def test_tier2_pyscf_energies_gpu():
+    """examples/08_rhf_tier2.py:33-41 through the CUDA path in the spherical
+    basis: the reference's own energies to 1e-8 Eh and, for water in STO-3G,
+    6-31G and 6-31G**, the PySCF energies to 1e-8 Eh."""
+    import json
+
+    data = json.load(open(os.path.join(GOLDEN, "tier2_pyscf.json")))
+    for key, d in data.items():
+        mol = make_molecule(tuple(d["elements"]), np.array(d["coords"], dtype=float), np.array(d["Z"]))
+        bs = pb.build_basis_set(mol, d["basis"], spherical=True)
+        assert bs.n_basis == d["n_basis"]
+        ints = compute_integrals(mol, bs, device=0, schwarz_tau=0.0)
+        res = run_scf(mol, ints, CalcConfig(scf_conv=1e-10))
+        assert res.converged, key
+        assert abs(res.energy - d["reference_energy"]) < 1e-8, key
+        if key.startswith("H2O/"):
+            assert abs(res.energy - d["golden_pyscf"]) < 1e-8, key

@@ -34,7 +34,7 @@ def _call(name, eng, D, J, K, prec, mixed_tau, dens_tau):
 @pytest.mark.parametrize("prec,dens_tau", [("fp64", 1e-11), ("mixed", 0.0)])
 def test_noalloc_matches_jk_twice(prec, dens_tau):
     mol = pb.water_cluster(3, seed=5)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     eng = DirectERI(bs, mol, device=0, schwarz_tau=1e-12)
     n = bs.n_basis
     rng = np.random.default_rng(11)
@@ -56,7 +56,7 @@ def test_noalloc_matches_jk_twice(prec, dens_tau):
 
 def test_noalloc_requires_prebuilt_work_list():
     mol = pb.water_cluster(1, seed=0)
-    bs = pb.build_basis_set(mol, "syn-6-31g*")
+    bs = pb.build_basis_set(mol, "6-31g*")
     eng = DirectERI(bs, mol, device=0, schwarz_tau=1e-12)
     n = bs.n_basis
     D = torch.eye(n, dtype=torch.float64, device="cuda:0")[None].contiguous()
@@ -64,4 +64,42 @@ def test_noalloc_requires_prebuilt_work_list():
     K = torch.empty_like(D)
     with pytest.raises(_abi.JQCError, match="work list"):
         _call("jqc_jk_noalloc", eng, D, J, K, "fp32", 1e-7, 0.0)
+    eng.close()
+
+
+def test_noalloc_leaves_device_memory_untouched():
+    """After the set-up call, repeated jqc_jk_noalloc calls change the
+    device's free memory by nothing (cudaMemGetInfo before and after)."""
+    mol = pb.water_cluster(2, seed=9)
+    bs = pb.build_basis_set(mol, "6-31g*")
+    eng = DirectERI(bs, mol, device=0, schwarz_tau=1e-12)
+    n = bs.n_basis
+    D = torch.eye(n, dtype=torch.float64, device="cuda:0")[None].contiguous() * 0.1
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    _call("jqc_jk", eng, D, J, K, "fp64", 1e-7, 1e-11)
+    _call("jqc_jk_noalloc", eng, D, J, K, "fp64", 1e-7, 1e-11)  # first call on the device: address look-up
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        _call("jqc_jk_noalloc", eng, D, J, K, "fp64", 1e-7, 1e-11)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    eng.close()
+
+
+def test_noalloc_rejects_more_shells_than_the_static_scratch():
+    """52 waters in 6-31G* have 520 shells, more than the 512 the static
+    scratch holds: the call fails with JQC_ERR_TOO_LARGE before it looks
+    for a work list or launches anything."""
+    mol = pb.water_cluster(52, seed=0)
+    bs = pb.build_basis_set(mol, "6-31g*")
+    assert len(bs.shells) == 520
+    eng = DirectERI(bs, mol, device=0, schwarz_tau=1e-10)
+    n = bs.n_basis
+    D = torch.zeros((1, n, n), dtype=torch.float64, device="cuda:0")
+    J = torch.empty_like(D)
+    K = torch.empty_like(D)
+    with pytest.raises(_abi.JQCTooLarge, match="static scratch"):
+        _call("jqc_jk_noalloc", eng, D, J, K, "fp64", 1e-7, 0.0)
     eng.close()
