@@ -406,10 +406,13 @@ class _BatchFock:
         self.kinds.append(("%s-%s" % (self._settings(inc)[0], "inc" if inc else "full"), len(dens)))
         return {m: (b.block(self.Jacc, m), b.block(self.Kacc, m)) for m in dens}
 
-    def observe(self, err_max: float) -> None:
+    def observe(self, err_max: float) -> bool:
+        """True when this call switched the batch from the mixed phase to FP64."""
         if self.phase == "mixed" and err_max < float(self.config.fp64_switch):
             self.phase = "fp64"
             self.prev = None  # next build: a full FP64 build
+            return True
+        return False
 
     def converged_ok(self) -> bool:
         return not self.mixed or (self.phase == "fp64" and self.fp64_builds >= int(self.config.fp64_tail_iters))
@@ -603,7 +606,10 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
         host = torch.cat([torch.cat(Es), torch.cat(emaxs)]).cpu().numpy()
         E_now, emax = host[:len(order)], host[len(order):]
         act_host = ~converged[order]
-        fb.observe(float(emax[act_host].max()) if act_host.any() else 0.0)
+        if fb.observe(float(emax[act_host].max()) if act_host.any() else 0.0) and config.diis_reset_at_switch:
+            for g in groups:  # as FockBuilder's drivers: no mixed-phase Fock matrix in the FP64 extrapolation
+                g.Fh.clear()
+                g.Eh.clear()
         ok = fb.converged_ok()
         for k, m in enumerate(order):
             if converged[m]:

@@ -152,6 +152,9 @@ class CalcConfig(_Replace):
                     unscreened).  0: 1e-11 saves ~1 ms on (H2O)16 but moved
                     the 64-cluster sweep's largest energy error from about
                     6.5e-7 to 7.1e-7 Eh, too close to the 1e-6 tolerance.
+    diis_reset_at_switch: clear the DIIS history when the mixed policy
+                    switches to FP64, so the extrapolated Fock matrix of the
+                    energy holds FP64 builds only.
     """
 
     method: str = "rhf"
@@ -174,6 +177,7 @@ class CalcConfig(_Replace):
     fp64_tail_dens_tau: float = 1e-11
     mixed_full_dens_tau: float = 1e-9
     fp64_switch_dens_tau: float = 0.0
+    diis_reset_at_switch: bool = True
 
 
 def make_molecule(elements, coords, atomic_numbers, charge: int = 0, spin: int = 0) -> Molecule:

@@ -51,16 +51,25 @@ constexpr int kBoysARow = 8;
 constexpr int kBoysExpOff = (kBoysMaxM + 1) * kBoysRows * kBoysARow;
 constexpr int kBoysAlignedSize = kBoysExpOff + kBoysExpRows;
 
+// 32-byte vector loads through the read-only data path (256-bit loads,
+// sm_100 and later); the address must be 32-byte aligned.  One load of a
+// 32-byte record is one L1 request where two 16-byte loads were two, which
+// matters for the scattered per-lane reads (table rows, primitive pairs) that
+// bound the low-L kernels.
+__device__ __forceinline__ void ldg32B(const double* __restrict__ p, double& a, double& b, double& c, double& d) {
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
+__device__ __forceinline__ void ldg32B(const float* __restrict__ p, float (&v)[8]) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+      : "l"(p));
+}
+
 __device__ __forceinline__ void boys_row(const double* __restrict__ r, double (&v)[8]) {
-  const double2* q = reinterpret_cast<const double2*>(r);
-  const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
-  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+  ldg32B(r, v[0], v[1], v[2], v[3]);
+  ldg32B(r + 4, v[4], v[5], v[6], v[7]);
 }
-__device__ __forceinline__ void boys_row(const float* __restrict__ r, float (&v)[8]) {
-  const float4* q = reinterpret_cast<const float4*>(r);
-  const float4 a = __ldg(q), b = __ldg(q + 1);
-  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-}
+__device__ __forceinline__ void boys_row(const float* __restrict__ r, float (&v)[8]) { ldg32B(r, v); }
 
 // Writes F_0 .. F_M at T into F[0..M] from the aligned table `tabA`.
 // e^{-t} comes from the tabulated e^{-T_i} for every t (0 beyond the end of

@@ -19,26 +19,30 @@ namespace jqc {
 
 // One primitive pair of a shell pair (a, b): p = alpha + beta,
 // P = (alpha A + beta B) / p, K = exp(-alpha beta |AB|^2 / p) c_a c_b,
-// h = 1/(2p) (kept so no kernel divides by p).
-struct __align__(16) PrimPair {
+// h = 1/(2p) (kept so no kernel divides by p).  32-byte aligned: the records
+// live in cudaMalloc'd arrays and are read with 32-byte vector loads.
+struct __align__(32) PrimPair {
   double p, h, Px, Py, Pz, K, alpha, beta;
 };
-struct __align__(16) PrimPairF {
+struct __align__(32) PrimPairF {
   float p, h, Px, Py, Pz, K, alpha, beta;
 };
+static_assert(sizeof(PrimPair) == 64 && sizeof(PrimPairF) == 32, "primitive-pair records");
 
-// 16-byte vector loads of a primitive-pair record through the read-only path
+// 32-byte vector loads of a primitive-pair record through the read-only path
 // (global memory only; records built in registers/local memory are read
 // with plain loads, see quartet_accumulate's GLOBAL_PP).
 __device__ __forceinline__ PrimPair ld_pp(const PrimPair* q) {
-  const double2* v = reinterpret_cast<const double2*>(q);
-  const double2 a = __ldg(v), b = __ldg(v + 1), c = __ldg(v + 2), d = __ldg(v + 3);
-  return PrimPair{a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y};
+  const double* v = reinterpret_cast<const double*>(q);
+  PrimPair r;
+  ldg32B(v, r.p, r.h, r.Px, r.Py);
+  ldg32B(v + 4, r.Pz, r.K, r.alpha, r.beta);
+  return r;
 }
 __device__ __forceinline__ PrimPairF ld_pp(const PrimPairF* q) {
-  const float4* v = reinterpret_cast<const float4*>(q);
-  const float4 a = __ldg(v), b = __ldg(v + 1);
-  return PrimPairF{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  float v[8];
+  ldg32B(reinterpret_cast<const float*>(q), v);
+  return PrimPairF{v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
 }
 template <typename T>
 struct PPType;

@@ -238,8 +238,13 @@ class DirectERI:
         with torch.cuda.device(self.device):
             _abi.call("jqc_eri_tensor", self._ctx, _ptr(out), int(max_bytes), _stream(self.device))
         if self._C is not None:
+            # one index at a time (a single four-operand einsum may contract
+            # the C factors with each other first, an n^8 intermediate)
             C = self._C
-            out = torch.einsum("Ii,Jj,Kk,Ll,ijkl->IJKL", C, C, C, C, out)
+            out = torch.tensordot(C, out, dims=([1], [0]))
+            out = torch.tensordot(C, out, dims=([1], [1])).transpose(0, 1)
+            out = torch.tensordot(out, C, dims=([2], [1])).transpose(2, 3)
+            out = torch.tensordot(out, C, dims=([3], [1])).contiguous()
         return out
 
     def one_electron(self):

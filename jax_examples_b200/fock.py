@@ -25,7 +25,11 @@ the precision policy of the mixed path:
   about 1e-7 Eh of the plain FP64 energy; the full rebuild at the switch is
   what keeps it there, without it the mixed-phase errors stay at 1e-5 Eh),
   and convergence is only accepted after ``fp64_tail_iters`` of them: the
-  final energy is an FP64 energy.
+  final energy is an FP64 energy.  The SCF drivers clear their DIIS history
+  at the switch (``diis_reset_at_switch``): the reported energy uses the
+  extrapolated Fock matrix (``rhf.py:80-81``), which would otherwise keep
+  mixing in mixed-phase Fock matrices and their FP32 and screening errors
+  (up to 1.6e-6 Eh in the 64-cluster sweep).
 """
 
 from __future__ import annotations
@@ -183,12 +187,15 @@ class FockBuilder:
         return H + Jt - K[0], H + Jt - K[1]
 
     # --------------------------------------------------------------- policy
-    def observe(self, err_max: float) -> None:
-        """Called once per SCF iteration with max|DIIS error|."""
+    def observe(self, err_max: float) -> bool:
+        """Called once per SCF iteration with max|DIIS error|; True when this
+        call switched the builder from the mixed phase to FP64."""
         if self.phase == "mixed" and err_max < self.fp64_switch:
             self.phase = "fp64"
             self.switched = True
             self._prev = None  # next build is a full FP64 build
+            return True
+        return False
 
     def converged_ok(self) -> bool:
         if self.precision != "mixed" or not self.direct:

@@ -60,6 +60,10 @@ class DIIS:
         self.F = []
         self.E = []
 
+    def clear(self) -> None:
+        self.F.clear()
+        self.E.clear()
+
     def push(self, F, e):
         self.F.append(F)
         self.E.append(e)
@@ -149,7 +153,8 @@ def run_rhf(mol, ints, config: Optional[CalcConfig] = None, timer: Optional[Stag
             dE = abs(E - last)
             err_max = float(torch.max(torch.abs(err)))
             last = E
-            fb.observe(err_max)
+            if fb.observe(err_max) and config.diis_reset_at_switch:
+                diis.clear()  # the extrapolated F (and E) must not mix in the mixed-phase Fock matrices
             if dE < config.scf_conv and err_max < max(config.scf_conv, 1e-6) and fb.converged_ok():
                 converged = True
                 break
@@ -218,7 +223,8 @@ def run_uhf(mol, ints, config: Optional[CalcConfig] = None, timer: Optional[Stag
             err = max(float(torch.max(torch.abs(e_a))), float(torch.max(torch.abs(e_b))))
             dE = abs(E - last)
             last = E
-            fb.observe(err)
+            if fb.observe(err) and config.diis_reset_at_switch:
+                diis.clear()
             if dE < config.scf_conv and err < max(config.scf_conv, 1e-6) and fb.converged_ok():
                 converged = True
                 break
