@@ -38,9 +38,28 @@ __device__ __forceinline__ float boys_rsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ int boys_round(double x) { return __double2int_rn(x); }
 __device__ __forceinline__ int boys_round(float x) { return __float2int_rn(x); }
 
+template <typename T>
+struct RoundMagic;
+template <>
+struct RoundMagic<double> {
+  static constexpr double value = 6755399441055744.0;  // 1.5 * 2^52
+  static __device__ __forceinline__ int low(double x) { return __double2loint(x); }
+};
+template <>
+struct RoundMagic<float> {
+  static constexpr float value = 12582912.0f;  // 1.5 * 2^23
+  static __device__ __forceinline__ int low(float x) { return __float_as_int(x) - 0x4B400000; }
+};
+
+__host__ __device__ constexpr double inv_factorial(int k) {
+  double f = 1.0;
+  for (int j = 2; j <= k; ++j) f *= j;
+  return 1.0 / f;
+}
+
 // Aligned per-order table used by the hot kernels: for order M and grid
-// point i the 8 values F_{M+k}(T_i), k < 8, are one 64-byte (FP64) or 32-byte
-// (FP32) aligned row at tabA[(M * kBoysRows + i) * 8], fetched with 16-byte
+// point i the 8 values F_{M+k}(T_i) / k!, k < 8, are one 64-byte (FP64) or
+// 32-byte (FP32) aligned row at tabA[(M * kBoysRows + i) * 8], fetched with 16-byte
 // vector loads.
 constexpr int kBoysARow = 8;
 // After the (kBoysMaxM+1) x kBoysRows rows of the aligned table come the
@@ -79,23 +98,28 @@ template <typename T, int M>
 __device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F)[M + 1]) {
   constexpr int KT = BoysConst<T>::kTaylor;
   const T tc = t < T(kBoysExpTEnd) ? t : T(kBoysExpTEnd);
-  const int i = boys_round(tc * T(kBoysGridInv));
-  const T d = T(i) * T(1.0 / kBoysGridInv) - tc;  // T_i - t, |d| <= 1/32
+  // i = round(16 tc) without conversion instructions: adding 1.5 * 2^52
+  // (2^23 in FP32) to 0 <= x < 2^22 leaves round-to-nearest(x) in the low
+  // mantissa bits, and subtracting it again gives that integer exactly.
+  const T xr = tc * T(kBoysGridInv) + RoundMagic<T>::value;
+  const int i = RoundMagic<T>::low(xr);
+  const T d = (xr - RoundMagic<T>::value) * T(1.0 / kBoysGridInv) - tc;  // T_i - t, |d| <= 1/32
   T e = T(0);
   if constexpr (M > 0) {
-    // e^{-t} = e^{-T_i} e^{d}; the series of e^{d} to KT terms is as accurate
-    // as the Taylor series of F below
-    T ed = T(1);
+    // e^{-t} = e^{-T_i} e^{d}, e^d by Horner over the coefficients 1/k!
+    T ed = T(inv_factorial(KT - 1));
 #pragma unroll
-    for (int k = KT - 1; k >= 1; --k) ed = T(1) + ed * (d * T(1.0 / k));
+    for (int k = KT - 2; k >= 0; --k) ed = ed * d + T(inv_factorial(k));
     e = __ldg(tabA + kBoysExpOff + i) * ed;
   }
   if (t < T(kBoysTMax)) {
+    // the row holds F_{M+k}(T_i) / k!: the Taylor series in d is a Horner
+    // chain of fused multiply-adds
     T v[8];
     boys_row(tabA + (M * kBoysRows + i) * kBoysARow, v);
     T acc = v[KT - 1];
 #pragma unroll
-    for (int k = KT - 2; k >= 0; --k) acc = v[k] + acc * (d * T(1.0 / (k + 1)));
+    for (int k = KT - 2; k >= 0; --k) acc = acc * d + v[k];
     F[M] = acc;
     if constexpr (M > 0) {
       const T t2 = t + t;

@@ -130,7 +130,7 @@ int boys_tables_all(int device, BoysTables* out) {
     for (int M = 0; M <= kBoysMaxM; ++M)
       for (int i = 0; i < kBoysRows; ++i)
         for (int k = 0; k < kBoysARow; ++k)
-          ha[((size_t)M * kBoysRows + i) * kBoysARow + k] = h[(size_t)i * kBoysCols + M + k];
+          ha[((size_t)M * kBoysRows + i) * kBoysARow + k] = h[(size_t)i * kBoysCols + M + k] * inv_factorial(k);
     for (int i = 0; i < kBoysExpRows; ++i) ha[kBoysExpOff + i] = (double)expl(-(long double)i / kBoysGridInv);
     std::vector<float> haf(ha.begin(), ha.end());
     int prev = 0;
