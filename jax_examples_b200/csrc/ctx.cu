@@ -1,6 +1,7 @@
 // Host side of libjqc.so: context, basis upload, shell-pair build with
 // Schwarz bounds, class-sorted work lists and the extern "C" entry points.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -458,55 +459,89 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
     }
     for (auto& th : pool) th.join();
   }
-  std::vector<Task> lists[2][kNumQuartetClasses];
   long long nq[2] = {0, 0}, npq = 0;
   long long cq[2][kNumQuartetClasses] = {}, cp[2][kNumQuartetClasses] = {};
-  for (int prec = 0; prec < 2; ++prec)
-    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-      size_t total = 0;
-      for (const TaskPart& p : parts) total += p.lists[prec][qc].size();
-      lists[prec][qc].reserve(total);
-      for (TaskPart& p : parts) {
-        lists[prec][qc].insert(lists[prec][qc].end(), p.lists[prec][qc].begin(), p.lists[prec][qc].end());
-        cq[prec][qc] += p.cq[prec][qc];
-        cp[prec][qc] += p.cp[prec][qc];
-      }
-    }
   for (const TaskPart& p : parts) {
     nq[0] += p.nq[0];
     nq[1] += p.nq[1];
     npq += p.npq;
+    for (int prec = 0; prec < 2; ++prec)
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+        cq[prec][qc] += p.cq[prec][qc];
+        cp[prec][qc] += p.cp[prec][qc];
+      }
   }
-  // Longest tasks first inside each class launch (cost = lane primitive
-  // quartets = bra primitive chunk x ket primitive pairs): a stable counting
-  // sort on the cost, linear in the number of tasks.
+  // Every (precision path, class) list is finished on its own, the lists in
+  // parallel: the parts are concatenated in bra order, the tasks ordered
+  // longest first (cost = lane primitive quartets = bra primitive chunk x
+  // ket primitive pairs; a stable counting sort, linear in the number of
+  // tasks), and the ket-outer register classes packed into warp groups.
+  constexpr int kSegs = 2 * kNumQuartetClasses;
+  std::vector<std::vector<Task>> seg_tasks(kSegs);
+  std::vector<std::vector<int>> seg_groups(kSegs);
+  std::vector<int> seg_ngroups(kSegs, 0);
+  auto finish_segment = [&](int sg) {
+    const int prec = sg / kNumQuartetClasses, qc = sg % kNumQuartetClasses;
+    size_t total = 0;
+    for (const TaskPart& p : parts) total += p.lists[prec][qc].size();
+    std::vector<int> cost(total), count;
+    int cmax = 0;
+    {
+      size_t k = 0;
+      for (const TaskPart& p : parts)
+        for (const Task& t : p.lists[prec][qc]) {
+          cost[k] = ((t.flags >> 16) - (t.flags & 0xffff)) * c->pairs[t.ket0].npp;
+          cmax = std::max(cmax, cost[k]);
+          ++k;
+        }
+    }
+    count.assign(cmax + 2, 0);
+    for (size_t k = 0; k < total; ++k) ++count[cmax - cost[k] + 1];  // descending cost
+    for (int b = 1; b <= cmax + 1; ++b) count[b] += count[b - 1];
+    std::vector<Task>& out = seg_tasks[sg];
+    out.resize(total);
+    {
+      size_t k = 0;
+      for (const TaskPart& p : parts)
+        for (const Task& t : p.lists[prec][qc]) out[count[cmax - cost[k++]]++] = t;
+    }
+    if (!full && !grad && qc_bra_lsum(qc) <= kKetOuterMaxLab && class_engine(c->tune[qc], qc) == kEngineReg)
+      seg_ngroups[sg] = pack_groups(out, 0, total, seg_groups[sg], [c](const Task& t) {
+        return ((t.flags >> 16) - (t.flags & 0xffff)) * c->pairs[t.ket0].npp;
+      });
+  };
+  {
+    std::vector<std::thread> pool;
+    std::atomic<int> next{0};
+    const int nw = std::max(1, std::min(nthreads, kSegs));
+    for (int w = 0; w < nw; ++w)
+      pool.emplace_back([&]() {
+        for (int sg = next++; sg < kSegs; sg = next++) finish_segment(sg);
+      });
+    for (auto& th : pool) th.join();
+  }
+  parts.clear();
   ts.h.clear();
   ts.gh.clear();
-  std::vector<int> cost, count;
-  for (int prec = 0; prec < 2; ++prec)
-    for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
-      const auto& v = lists[prec][qc];
-      ts.off[prec][qc] = (int)ts.h.size();
-      ts.cnt[prec][qc] = (int)v.size();
-      cost.resize(v.size());
-      int cmax = 0;
-      for (size_t k = 0; k < v.size(); ++k) {
-        cost[k] = ((v[k].flags >> 16) - (v[k].flags & 0xffff)) * c->pairs[v[k].ket0].npp;
-        cmax = std::max(cmax, cost[k]);
-      }
-      count.assign(cmax + 2, 0);
-      for (size_t k = 0; k < v.size(); ++k) ++count[cmax - cost[k] + 1];  // descending cost
-      for (int b = 1; b <= cmax + 1; ++b) count[b] += count[b - 1];
-      const size_t base = ts.h.size();
-      ts.h.resize(base + v.size());
-      for (size_t k = 0; k < v.size(); ++k) ts.h[base + count[cmax - cost[k]]++] = v[k];
-      ts.goff[prec][qc] = (int)ts.gh.size();
-      ts.gcnt[prec][qc] = 0;
-      if (!full && !grad && qc_bra_lsum(qc) <= kKetOuterMaxLab && class_engine(c->tune[qc], qc) == kEngineReg)
-        ts.gcnt[prec][qc] = pack_groups(ts.h, base, v.size(), ts.gh, [c](const Task& t) {
-          return ((t.flags >> 16) - (t.flags & 0xffff)) * c->pairs[t.ket0].npp;
-        });
-    }
+  size_t total_tasks = 0, total_groups = 0;
+  for (int sg = 0; sg < kSegs; ++sg) {
+    total_tasks += seg_tasks[sg].size();
+    total_groups += seg_groups[sg].size();
+  }
+  ts.h.resize(total_tasks);
+  ts.gh.reserve(total_groups);
+  size_t base = 0;
+  for (int sg = 0; sg < kSegs; ++sg) {
+    const int prec = sg / kNumQuartetClasses, qc = sg % kNumQuartetClasses;
+    ts.off[prec][qc] = (int)base;
+    ts.cnt[prec][qc] = (int)seg_tasks[sg].size();
+    std::copy(seg_tasks[sg].begin(), seg_tasks[sg].end(), ts.h.begin() + (long)base);
+    base += seg_tasks[sg].size();
+    ts.goff[prec][qc] = (int)ts.gh.size();
+    ts.gcnt[prec][qc] = seg_ngroups[sg];
+    ts.gh.insert(ts.gh.end(), seg_groups[sg].begin(), seg_groups[sg].end());
+    std::vector<Task>().swap(seg_tasks[sg]);
+  }
   JQC_CUDA_CHECK(ts.d.upload(ts.h, s));
   JQC_CUDA_CHECK(ts.gd.upload(ts.gh, s));
   ts.n_quartets[0] = nq[0];
