@@ -49,6 +49,20 @@ def shard_by_cost(costs: Sequence[float], rank: int, world: int) -> List[int]:
     return list(range(bounds[rank], bounds[rank + 1]))
 
 
+def sweep_cost(n_waters: int) -> float:
+    """Estimated cost of one water cluster's energy and gradient: the
+    surviving quartets of a lattice cluster grow about as n^2.5 at 1..12
+    waters."""
+    return float(n_waters) ** 2.5
+
+
+def sweep_shard(sizes: Sequence[int], rank: int, world: int) -> List[int]:
+    """Molecules (indices into ``sizes``, waters per cluster) that ``rank``
+    evaluates in a sweep sharded over ``world`` GPUs: contiguous and
+    balanced by :func:`sweep_cost`, every molecule on exactly one rank."""
+    return shard_by_cost([sweep_cost(n) for n in sizes], rank, world)
+
+
 def _reduce_device() -> torch.device:
     if dist.get_backend() == "nccl":
         return torch.device("cuda", torch.cuda.current_device())

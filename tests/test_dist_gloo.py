@@ -12,7 +12,9 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from jax_examples_b200.dist import max_over_ranks, shard_by_cost, sum_over_ranks
+import numpy as np
+
+from jax_examples_b200.dist import max_over_ranks, shard_by_cost, sum_over_ranks, sweep_cost, sweep_shard
 
 
 def _free_port() -> int:
@@ -28,6 +30,21 @@ def _worker(rank: int, world: int, port: int, costs, out):
         mine = shard_by_cost(costs, rank, world)
         work = sum(costs[i] for i in mine)
         out[rank] = (mine, max_over_ranks(float(rank + 1) * 1.5), sum_over_ranks(work))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def _sweep_worker(rank: int, world: int, port: int, out):
+    """What bench.py's sharded sweep does before it touches a GPU: the seeded
+    64-cluster sizes, this rank's share, and the reductions of its timings."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sizes = [int(x) for x in np.random.default_rng(2024).integers(1, 13, 64)]
+        mine = sweep_shard(sizes, rank, world)
+        cost = sum(sweep_cost(sizes[i]) for i in mine)
+        out[rank] = (sizes, mine, cost, max_over_ranks(cost), sum_over_ranks(float(len(mine))))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -58,3 +75,20 @@ def test_shard_by_cost_edge_cases():
     with pytest.raises(ValueError):
         shard_by_cost([1.0], 2, 2)
     assert max_over_ranks(2.5) == 2.5  # no process group: identity
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sweep_sharded_over_gloo_ranks(world):
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.start_processes(_sweep_worker, args=(world, _free_port(), out), nprocs=world, start_method="spawn")
+        res = dict(out)
+    sizes = res[0][0]
+    shards = [res[r][1] for r in range(world)]
+    assert sum(shards, []) == list(range(len(sizes)))  # contiguous, in order, each molecule once
+    total = sum(sweep_cost(n) for n in sizes)
+    for r in range(world):
+        assert res[r][3] == pytest.approx(max(res[q][2] for q in range(world)))
+        assert res[r][4] == pytest.approx(len(sizes))
+        # balanced to within one molecule's cost
+        assert abs(res[r][2] - total / world) <= max(sweep_cost(n) for n in sizes)
