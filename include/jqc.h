@@ -95,6 +95,19 @@ int jqc_set_geometry(jqc_ctx *ctx, const double *atom_xyz);
  * molecule). */
 int jqc_set_molecule_mask(jqc_ctx *ctx, const int *active);
 
+/* Molecule activity read on the device by every later J/K build of a batch
+ * context (jqc_batch_partition with more than one molecule), graph replays
+ * included: d_active points to n_mol ints in device memory, owned by the
+ * caller, who may rewrite them between builds (a converged molecule of a
+ * lock-step SCF gets 0).  Each build first compacts the class work lists on
+ * the device to the work items holding a task of an active molecule, and the
+ * class kernels walk only those (the register kernels as persistent grids
+ * over the device-side counts); the J and K blocks of inactive molecules
+ * come out zero.  NULL switches it off.  Captured graphs are dropped when the
+ * pointer changes.  No reference counterpart (scf/rhf.py:95-169 runs one
+ * molecule). */
+int jqc_set_molecule_activity(jqc_ctx *ctx, const int *d_active);
+
 /* Counters of the work list for (precision_mode, mixed_tau) as jqc_jk
  * would use it: out[0] shell pairs, out[1] kept pairs, out[2] screened
  * canonical quartets on the FP64 path, out[3] on the FP32 path, out[4]

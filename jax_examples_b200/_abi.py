@@ -72,6 +72,7 @@ SIGNATURES = {
     "jqc_batch_partition": (_c_int, [_vp, _c_int, _ip]),
     "jqc_set_geometry": (_c_int, [_vp, _dp]),
     "jqc_set_molecule_mask": (_c_int, [_vp, _ip]),
+    "jqc_set_molecule_activity": (_c_int, [_vp, _vp]),
     "jqc_grad2e_ex": (_c_int, [_vp, _c_int, _vp, _c_dbl, _c_dbl, _c_dbl, _vp, _vp, _dp]),
     "jqc_set_grad_engine": (_c_int, [_vp, _c_int, _c_int]),
     "jqc_get_grad_engine": (_c_int, [_vp, _ip]),

@@ -46,10 +46,11 @@ from .integrals import nuclear_repulsion_energy
 # 1e-30 Eh: the builds stay FP64-exact for every active molecule.
 BATCH_DENS_TAU = 1e-30
 
-# Density screening of the gradient on the mixed path: the skipped quartets
-# change a (H2O)16 gradient by ~3.5e-6 Eh/bohr (1e-10: 1e-6, 1e-9: 1e-5),
-# inside the 1e-5 tolerance, for 38 ms instead of 75 ms unscreened.
-MIXED_GRAD_TAU = 3e-10
+# Density screening of the gradient on the mixed path: on (H2O)16 6-31G* the
+# skipped quartets change the gradient by 3.0e-6 Eh/bohr (3e-10: 9.8e-7,
+# 3e-9: 9.6e-6), a 3x margin to the 1e-5 tolerance, for 16.5 ms instead of
+# 41.8 ms unscreened; the 64-cluster sweep's largest change is 2.5e-6.
+MIXED_GRAD_TAU = 1e-9
 
 
 class _Nuclei:
@@ -308,6 +309,23 @@ class _BatchFock:
         self.D, self.J, self.K = eng.buffers(1)
         self.Jacc = torch.zeros_like(self.J[0])
         self.Kacc = torch.zeros_like(self.K[0])
+        # molecules of the next build, read on the device by every build and
+        # graph replay: the others are compacted out of the work lists
+        self.n_mol = eng.engine.n_mol
+        self.active = None
+        if self.cart and self.n_mol > 1:
+            self.active = torch.ones(self.n_mol, dtype=torch.int32, device=eng.device)
+            self._active_host = np.ones(self.n_mol, dtype=np.int32)
+            eng.engine.set_molecule_activity(self.active)
+
+    def _set_active(self, molecules) -> None:
+        if self.active is None:
+            return
+        mask = np.zeros(self.n_mol, dtype=np.int32)
+        mask[list(molecules)] = 1
+        if not np.array_equal(mask, self._active_host):
+            self._active_host = mask
+            self.active.copy_(torch.from_numpy(mask))
 
     def _settings(self, incremental: bool, phase: Optional[str] = None):
         """(precision, density-screening threshold) of the next build."""
@@ -342,6 +360,7 @@ class _BatchFock:
         """Work lists, autotuning and graph capture before the timed builds."""
         if not self.cart:
             return
+        self._set_active(dens.keys())
         for m, d in dens.items():
             self.batch.block(self.D[0], m).copy_(d)
         prec, tau = self._settings(False)
@@ -383,6 +402,7 @@ class _BatchFock:
         # same largest energy error)
         periodic = not self.switched and self.since_full >= self.rebuild_every
         inc = self.incremental and self.prev is not None and not periodic and set(dens) <= set(self.prev)
+        self._set_active(dens.keys())
         self.D.zero_()
         if inc:
             for m, d in dens.items():

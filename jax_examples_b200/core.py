@@ -134,6 +134,9 @@ class CalcConfig(_Replace):
                     (H2O)16 the mixed builds are ~7% faster than at 1e-7 with
                     the same iterations and final error; 1e-2 and above cost
                     extra SCF iterations).
+    fp64_switch:    max|DIIS error| below which the mixed policy switches to
+                    FP64 (1e-4: 25-26 iterations on (H2O)16 instead of 28 at
+                    1e-5, with the DIIS history cleared at the switch).
     fp64_tail_iters: in mixed mode, once the SCF is within ``fp64_switch`` of
                     convergence the remaining iterations use incremental FP64
                     builds; at least this many FP64 iterations are run.
@@ -142,16 +145,18 @@ class CalcConfig(_Replace):
                     in the mixed phase.
     fp64_tail_dens_tau: density-screening threshold of the incremental FP64
                     builds after the switch (mixed mode only; plain FP64
-                    incremental builds screen at 1e-12).  1e-11: at 1e-10 the
-                    64-cluster sweep's largest energy error reached 7.6e-7 Eh
-                    (3.0e-7 at 1e-12, with no slower Fock builds there).
+                    incremental builds screen at 1e-12).
     mixed_full_dens_tau: density-screening threshold of the full builds of
                     the mixed phase (their errors are dropped at the switch).
     fp64_switch_dens_tau: density-screening threshold of the full FP64 build
                     at the switch (mixed mode only; plain FP64 builds are
-                    unscreened).  0: 1e-11 saves ~1 ms on (H2O)16 but moved
-                    the 64-cluster sweep's largest energy error from about
-                    6.5e-7 to 7.1e-7 Eh, too close to the 1e-6 tolerance.
+                    unscreened).
+                    The five thresholds were swept together on (H2O)16 and
+                    the 64-cluster sweep in 6-31G*, against FP64 converged
+                    to 1e-10: these defaults give 80.3 ms of Fock builds on
+                    (H2O)16 (88.4 ms with the previous 1e-5 / 1e-8 / 1e-11 /
+                    1e-9 / 0) at 5.6e-8 Eh, and the sweep's largest error
+                    1.9e-7 Eh (4.0e-8 before) in 0.67 s instead of 0.76 s.
     diis_reset_at_switch: clear the DIIS history when the mixed policy
                     switches to FP64, so the extrapolated Fock matrix of the
                     energy holds FP64 builds only.
@@ -171,12 +176,12 @@ class CalcConfig(_Replace):
     schwarz_tau: float = 1e-13
     mixed_tau: float = 1e-4
     fp64_tail_iters: int = 2
-    fp64_switch: float = 1e-5
+    fp64_switch: float = 1e-4
     incremental: bool = True
-    mixed_dens_tau: float = 1e-8
-    fp64_tail_dens_tau: float = 1e-11
-    mixed_full_dens_tau: float = 1e-9
-    fp64_switch_dens_tau: float = 0.0
+    mixed_dens_tau: float = 2e-8
+    fp64_tail_dens_tau: float = 1e-10
+    mixed_full_dens_tau: float = 1e-8
+    fp64_switch_dens_tau: float = 1e-11
     diis_reset_at_switch: bool = True
 
 

@@ -159,8 +159,12 @@ __global__ void __launch_bounds__(32 * kColWarps) col_jk_kernel(const JKParams p
   extern __shared__ __align__(16) unsigned char col_smraw[];
   S* sm = reinterpret_cast<S*>(col_smraw) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (warp >= prm.n_tasks) return;
+  if (prm.items != nullptr) {  // compacted work: the grid covers the whole list
+    if (warp >= *prm.n_items) return;
+    warp = prm.items[warp];
+  }
   // E entries beyond t = i + j are never written by ecoef_compute: zero them once
   for (int i = lane; i < int(sizeof(sm->Fk) / sizeof(T)); i += 32) (&sm->Fk[0][0][0][0])[i] = T(0);
   for (int i = lane; i < int(sizeof(sm->Eb) / sizeof(T)); i += 32) (&sm->Eb[0][0][0][0])[i] = T(0);

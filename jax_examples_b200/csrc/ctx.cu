@@ -183,6 +183,17 @@ struct TaskSet {
   long long n_prim_quartets = 0;
   long long class_quartets[2][kNumQuartetClasses] = {};
   long long class_prims[2][kNumQuartetClasses] = {};
+  // molecule compaction (batch contexts): one segment per non-empty list,
+  // the surviving item indices of segment k at d_items + comp_item_off[k]
+  bool comp_ready = false;
+  int comp_nseg = 0;
+  long long comp_total = 0;
+  int comp_seg_of[2][kNumQuartetClasses] = {};  // segment of a list, -1 none
+  long long comp_item_off[2 * kNumQuartetClasses] = {};
+  DevBuf<int> d_items;
+  DevBuf<int> d_counts;
+  DevBuf<CompactSeg> d_segs;
+  DevBuf<long long> d_seg_start;
 };
 
 // Pairs of one (class, primitive-pair count, molecule), Q descending.
@@ -251,6 +262,7 @@ struct jqc_ctx {
   int n_mol = 1;
   std::vector<int> shell_mol, atom_mol;
   std::vector<int> mol_active;  // empty: every molecule takes part in the pair list
+  const int* d_mol_active = nullptr;  // caller's device flags read by every J/K build (nullptr: off)
   DevBuf<int> d_shell_mol, d_atom_mol;
   // pairs (sorted: block by (class, K_a, K_b), Q descending inside)
   bool pairs_ready = false;
@@ -553,6 +565,47 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
   ts.mixed_tau = mixed_tau;
   ts.full = full;
   ts.valid = true;
+  // Batch contexts: segments for the device-side molecule compaction of the
+  // lists (used while jqc_set_molecule_activity is set).
+  ts.comp_ready = false;
+  if (c->n_mol > 1 && !full && !grad) {
+    std::vector<CompactSeg> segs;
+    std::vector<long long> starts;
+    long long tot = 0;
+    int nseg = 0;
+    for (int prec = 0; prec < 2; ++prec)
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+        ts.comp_seg_of[prec][qc] = -1;
+        const int items = ts.gcnt[prec][qc] > 0 ? ts.gcnt[prec][qc] : ts.cnt[prec][qc];
+        if (ts.cnt[prec][qc] == 0) continue;
+        ts.comp_seg_of[prec][qc] = nseg;
+        ts.comp_item_off[nseg] = tot;
+        starts.push_back(tot);
+        segs.push_back(CompactSeg{nullptr, nullptr, items, nullptr, nullptr});
+        tot += items;
+        ++nseg;
+      }
+    starts.push_back(tot);
+    JQC_CUDA_CHECK(ts.d_items.reserve((size_t)std::max<long long>(tot, 1)));
+    JQC_CUDA_CHECK(ts.d_counts.reserve((size_t)std::max(nseg, 1)));
+    int k = 0;
+    for (int prec = 0; prec < 2; ++prec)
+      for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
+        if (ts.comp_seg_of[prec][qc] < 0) continue;
+        CompactSeg& sg = segs[k];
+        sg.tasks = ts.d.ptr + ts.off[prec][qc];
+        sg.groups = ts.gcnt[prec][qc] > 0 ? ts.gd.ptr + ts.goff[prec][qc] : nullptr;
+        sg.out = ts.d_items.ptr + ts.comp_item_off[k];
+        sg.count = ts.d_counts.ptr + k;
+        ++k;
+      }
+    JQC_CUDA_CHECK(ts.d_segs.upload(segs, s));
+    JQC_CUDA_CHECK(ts.d_seg_start.upload(starts, s));
+    JQC_CUDA_CHECK(cudaStreamSynchronize(s));
+    ts.comp_nseg = nseg;
+    ts.comp_total = tot;
+    ts.comp_ready = true;
+  }
   return JQC_OK;
 }
 
@@ -641,6 +694,14 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
     JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, dmax, s));
   else
     dmax = nullptr;
+  // Molecules flagged inactive leave the build before any class kernel runs:
+  // the lists are compacted on the device.
+  const bool compact = c->d_mol_active != nullptr && ts->comp_ready && ts->comp_nseg > 0;
+  if (compact) {
+    JQC_CUDA_CHECK(cudaMemsetAsync(ts->d_counts.ptr, 0, (size_t)ts->comp_nseg * sizeof(int), s));
+    JQC_CUDA_CHECK(launch_compact(ts->d_segs.ptr, ts->d_seg_start.ptr, ts->comp_nseg, ts->comp_total,
+                                  c->d_pairs.ptr, c->d_shell_mol.ptr, c->d_mol_active, s));
+  }
   if (!class_ms) {
     JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
     for (int i = 0; i < kNumStreams; ++i) JQC_CUDA_CHECK(cudaStreamWaitEvent(c->side[i], c->ev_fork, 0));
@@ -672,6 +733,13 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
       if (ts->gcnt[prec][qc] > 0 && p.engine == kEngineReg) {
         p.groups = ts->gd.ptr + ts->goff[prec][qc];
         p.n_groups = ts->gcnt[prec][qc];
+      }
+      if (compact && ts->comp_seg_of[prec][qc] >= 0) {
+        const int sg = ts->comp_seg_of[prec][qc];
+        p.items = ts->d_items.ptr + ts->comp_item_off[sg];
+        p.n_items = ts->d_counts.ptr + sg;
+        p.shell_mol = c->d_shell_mol.ptr;
+        p.mol_active = c->d_mol_active;
       }
       if (class_ms) {
         JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));
@@ -877,6 +945,20 @@ int jqc_set_geometry(jqc_ctx* c, const double* atom_xyz) {
   drop_jk_tasks(c);
   c->full_tasks.valid = false;
   c->grad_tasks.valid = false;
+  return JQC_OK;
+}
+
+int jqc_set_molecule_activity(jqc_ctx* c, const int* d_active) {
+  JQC_REQUIRE(c != nullptr, JQC_ERR_INVALID, "jqc_set_molecule_activity: null context");
+  if (d_active != nullptr) {
+    cudaPointerAttributes attr;
+    const cudaError_t e = cudaPointerGetAttributes(&attr, d_active);
+    (void)cudaGetLastError();
+    JQC_REQUIRE(e == cudaSuccess && (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged),
+                JQC_ERR_INVALID, "jqc_set_molecule_activity: the flags must be in device memory");
+  }
+  if (d_active != c->d_mol_active) drop_graphs(c);  // graphs read the array they were captured with
+  c->d_mol_active = d_active;
   return JQC_OK;
 }
 

@@ -1,4 +1,6 @@
 // ERI-tensor, Schwarz, primitive-quartet and Boys kernels plus small helpers.
+#include <algorithm>
+
 #include "jk_impl.cuh"
 
 namespace jqc {
@@ -208,6 +210,66 @@ cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const i
                         cudaStream_t s) {
   const int tot = n_shell * n_shell;
   dmax_kernel<<<(tot + 255) / 256, 256, 0, s>>>(D, n_dens, n, n_shell, ao, l, dmax);
+  return cudaGetLastError();
+}
+
+// Molecule compaction of the work items of many lists at once: thread g takes
+// item g of the concatenated lists (segment by binary search on the prefix
+// sums), keeps it when one of its tasks belongs to an active molecule, and
+// the lanes of a warp that keep items of the same segment append them with
+// one atomic.  The order inside a segment follows the warps' progress.
+__global__ void __launch_bounds__(256) compact_kernel(const CompactSeg* __restrict__ segs,
+                                                      const long long* __restrict__ seg_start, int n_segs,
+                                                      long long total, const ShellPair* __restrict__ pairs,
+                                                      const int* __restrict__ shell_mol,
+                                                      const int* __restrict__ mol_active) {
+  const int lane = threadIdx.x & 31;
+  const long long step = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < total; base += step) {
+    const long long g = base + threadIdx.x;
+    int seg = -1, item = 0;
+    bool act = false;
+    if (g < total) {
+      int lo = 0, hi = n_segs - 1;  // last segment starting at or before g
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (seg_start[mid] <= g)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      seg = lo;
+      item = int(g - seg_start[seg]);
+      const CompactSeg S = segs[seg];
+      if (S.groups != nullptr) {
+        for (int t = S.groups[item]; t < S.groups[item + 1] && !act; ++t)
+          act = mol_active[shell_mol[pairs[S.tasks[t].bra].a]] != 0;
+      } else {
+        act = mol_active[shell_mol[pairs[S.tasks[item].bra].a]] != 0;
+      }
+    }
+    const unsigned same = __match_any_sync(0xffffffffu, act ? seg : -1);
+    if (act) {
+      const int leader = __ffs(same) - 1;
+      const int rank = __popc(same & ((1u << lane) - 1u));
+      int slot = 0;
+      if (lane == leader) slot = atomicAdd(segs[seg].count, __popc(same));
+      slot = __shfl_sync(same, slot, leader);
+      segs[seg].out[slot + rank] = item;
+    }
+  }
+}
+
+cudaError_t launch_compact(const CompactSeg* segs, const long long* seg_start, int n_segs, long long total_items,
+                           const ShellPair* pairs, const int* shell_mol, const int* mol_active, cudaStream_t s) {
+  if (total_items == 0 || n_segs == 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const long long want = (total_items + 255) / 256;
+  const int blocks = (int)std::min<long long>(want, (long long)sms * 8);
+  compact_kernel<<<blocks, 256, 0, s>>>(segs, seg_start, n_segs, total_items, pairs, shell_mol, mol_active);
   return cudaGetLastError();
 }
 

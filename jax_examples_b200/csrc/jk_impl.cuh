@@ -88,6 +88,8 @@ struct JKBody {
     const ShellPair bp = prm.pairs[task.bra];
     const ShellPair kp = prm.pairs[kidx];
     bool active = in_range;
+    // a compacted packed group may hold tasks of several molecules
+    if (kPacked && prm.items != nullptr && active) active = prm.mol_active[prm.shell_mol[bp.a]] != 0;
     if (prm.dmax != nullptr && active) {
       const float* dm = prm.dmax;
       const int ns = prm.n_shell;
@@ -223,8 +225,9 @@ __global__ void __launch_bounds__(kMaxJKThreads) jk_kernel(const JKParams prm) {
   constexpr int NS = class_split(LA, LB, LC, LD);
   __shared__ T sE[kMaxJKThreads / 32][3][LA + 1][LB + 1][LA + LB + 1];
   const int stride = int((gridDim.x * blockDim.x) >> 5);
-  const int n_work = prm.groups ? prm.n_groups : prm.n_tasks;
-  for (int warp = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); warp < n_work; warp += stride) {
+  const int n_work = prm.items ? *prm.n_items : (prm.groups ? prm.n_groups : prm.n_tasks);
+  for (int w = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); w < n_work; w += stride) {
+    const int warp = prm.items ? prm.items[w] : w;
     JKBody<T, LA, LB, LC, LD, NS> body{prm, warp, int(threadIdx.x & 31), sE[threadIdx.x >> 5]};
     dispatch_part<NS>(blockIdx.y, body);
     __syncwarp();  // every lane is done with the warp's bra E before the next task writes it
@@ -240,7 +243,7 @@ cudaError_t launch_jk_class(const JKParams& p, cudaStream_t s) {
   const int threads = (p.threads == 64 || p.threads == 256) ? p.threads : 128;
   const int wpb = threads / 32;
   long long blocks = ((p.groups ? p.n_groups : p.n_tasks) + wpb - 1) / wpb;
-  if (p.persistent) {
+  if (p.persistent || p.items != nullptr) {  // compacted work: the count is known on the device only
     // resident blocks per SM for this block size, times the SM count
     static int occ[3] = {0, 0, 0};
     static int sms = 0;

@@ -43,6 +43,27 @@ struct JKParams {
   // nullptr: one task per warp.
   const int* groups = nullptr;
   int n_groups = 0;
+  // Work compacted on the device: warp-sized work item w is items[w] (a
+  // group, or a task when there are no groups) for w < *n_items; the
+  // register kernels then run a persistent grid, the column and warp engines
+  // a grid over the whole list.  nullptr: every item.
+  const int* items = nullptr;
+  const int* n_items = nullptr;
+  // With items: molecule of each shell and the activity flags, so that the
+  // lanes of a packed group that hold an inactive molecule's task stay idle.
+  const int* shell_mol = nullptr;
+  const int* mol_active = nullptr;
+};
+
+// One (precision path, class) list for the molecule compaction: its tasks,
+// its warp groups (nullptr: one task per item), the item count and where
+// the surviving item indices and their count go.
+struct CompactSeg {
+  const Task* tasks;
+  const int* groups;
+  int n_items;
+  int* out;
+  int* count;
 };
 
 constexpr int kMaxJKThreads = 256;
@@ -90,6 +111,12 @@ cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool 
 cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
                         cudaStream_t s);
 cudaError_t launch_symmetrize(double* M, int count, int n, cudaStream_t s);
+// Writes, for every segment, the indices of the work items that hold a task
+// of an active molecule (mol_active[shell_mol[shell a of the bra pair]] != 0)
+// and their count (the counts must be zero on entry).  seg_start: n_segs + 1
+// prefix sums of the segments' item counts.
+cudaError_t launch_compact(const CompactSeg* segs, const long long* seg_start, int n_segs, long long total_items,
+                           const ShellPair* pairs, const int* shell_mol, const int* mol_active, cudaStream_t s);
 
 // Class tables: angular momenta of pair class pc.
 __host__ __device__ constexpr int pc_la(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : 2; }

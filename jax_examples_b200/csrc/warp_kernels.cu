@@ -37,9 +37,13 @@ template <typename T>
 __global__ void __launch_bounds__(kWarpBlock) warp_jk_kernel(const JKParams prm, int la, int lb, int lc, int ld) {
   using PPT = typename PPType<T>::type;
   WarpSmem<T>* sm = warp_smem<T>();
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= prm.n_tasks) return;
+  if (prm.items != nullptr) {  // compacted work: the grid covers the whole list
+    if (warp >= *prm.n_items) return;
+    warp = prm.items[warp];
+  }
   const Task task = prm.tasks[warp];
   const ShellPair bp = prm.pairs[task.bra];
   const PPT* pp = static_cast<const PPT*>(prm.pp);

@@ -169,6 +169,20 @@ class DirectERI:
         self.atom_xyz = xyz
         self.packed.centres = np.ascontiguousarray(xyz[self.packed.atom])
 
+    def set_molecule_activity(self, flags: Optional[torch.Tensor]) -> None:
+        """Device flags (int32, one per molecule of the batch partition) that
+        every later J/K build reads on the device: molecules flagged 0 are
+        compacted out of the work before the class kernels run
+        (``jqc_set_molecule_activity``).  ``None`` switches it off.  The
+        engine keeps a reference to the tensor; rewrite it in place."""
+        if flags is not None:
+            if not (flags.is_cuda and flags.dtype == torch.int32 and flags.is_contiguous()
+                    and flags.numel() == self.n_mol and flags.device == self.device):
+                raise ValueError(f"flags must be a contiguous int32 tensor of {self.n_mol} entries on {self.device}")
+        with torch.cuda.device(self.device):
+            _abi.call("jqc_set_molecule_activity", self._ctx, None if flags is None else _ptr(flags))
+        self._activity = flags
+
     # ------------------------------------------------------------ lifecycle
     def close(self) -> None:
         if getattr(self, "_ctx", None) is not None and self._ctx.value:

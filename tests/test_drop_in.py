@@ -82,7 +82,8 @@ def ref():
     drop_in.uninstall()
 
 
-@pytest.mark.parametrize("tag", ["water_synsto3g", "water_cation_synsto3g_uhf"])
+@pytest.mark.parametrize("tag", ["water_synsto3g", "water_cation_synsto3g_uhf", "water_sto3g",
+                                 "water_cation_sto3g_uhf"])
 def test_reference_scf_through_drop_in(ref, golden, tag):
     jax_qc, names = ref
     assert "jax_qc.scf.rhf.build_fock_rhf" in names and "jax_qc.scf.uhf.build_fock_uhf" in names

@@ -311,6 +311,47 @@ def test_geometry_update_and_molecule_mask_match_fresh_engines():
     eng.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_molecule_activity_compacts_builds(prec):
+    """jqc_set_molecule_activity: with molecule 1 of three flagged inactive
+    the build equals the full build on the active molecules' blocks (1e-12)
+    and leaves molecule 1's blocks zero; flags rewritten in place between two
+    replays of one captured graph select other molecules."""
+    mols = _mols([2, 1, 3], seed=51, noise=0.05)
+    batch = MoleculeBatch(mols, BASIS)
+    eng = BatchedERI(batch, schwarz_tau=1e-12)
+    rng = np.random.default_rng(52)
+    D = torch.tensor(_random_block_density(batch, rng), device=DEV)[None].contiguous()
+    J0, K0 = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J0, K0, prec, 1e-4)
+    flags = torch.tensor([1, 0, 1], dtype=torch.int32, device=DEV)
+    eng.engine.set_molecule_activity(flags)
+
+    def check(J, K, active):
+        for m in range(3):
+            o, k = batch.bf_off[m], batch.n_bf[m]
+            blk = (slice(o, o + k), slice(o, o + k))
+            if active[m]:
+                np.testing.assert_allclose(J[0][blk].cpu().numpy(), J0[0][blk].cpu().numpy(), atol=1e-12, rtol=0)
+                np.testing.assert_allclose(K[0][blk].cpu().numpy(), K0[0][blk].cpu().numpy(), atol=1e-12, rtol=0)
+            else:
+                assert float(J[0][blk].abs().max()) == 0.0 and float(K[0][blk].abs().max()) == 0.0
+
+    J, K = torch.empty_like(D), torch.empty_like(D)
+    eng.jk_into(D, J, K, prec, 1e-4)
+    check(J, K, [1, 0, 1])
+    gid = eng.capture_jk(D, J, K, prec, 1e-4, 0.0)
+    flags.copy_(torch.tensor([0, 1, 1], dtype=torch.int32))
+    J.fill_(float("nan"))
+    eng.launch(gid)
+    torch.cuda.synchronize()
+    check(J, K, [0, 1, 1])
+    eng.engine.set_molecule_activity(None)
+    eng.jk_into(D, J, K, prec, 1e-4)
+    check(J, K, [1, 1, 1])
+    eng.close()
+
+
 def _set_grad_engines(eng, engine, classes):
     for q in classes:
         _abi.call("jqc_set_grad_engine", eng._ctx, q, engine)
