@@ -111,3 +111,44 @@ def test_molecule_batch_layout():
     np.testing.assert_array_equal(blk.numpy(), M[38:57, 38:57])
     with pytest.raises(ValueError):
         jb.MoleculeBatch([], "6-31g*")
+
+
+def test_pooled_eigensolver_matches_per_matrix_eigh():
+    """The host eigensolver of the batched SCF: per member X^T F X solved on
+    the worker pool equals a plain eigh, for all members and for a subset
+    (the others come back as eps = 0, C = X)."""
+    import torch
+
+    rng = np.random.default_rng(7)
+    n_threads = torch.get_num_threads()
+
+    class G:
+        pass
+
+    groups, Fs = [], []
+    for n, m in [(19, 3), (38, 1), (57, 4)]:
+        S = rng.standard_normal((m, n, n))
+        S = S @ S.transpose(0, 2, 1) / n + np.eye(n)
+        w, U = np.linalg.eigh(S)
+        g = G()
+        g.X = torch.tensor(U * (1.0 / np.sqrt(w))[:, None, :] @ U.transpose(0, 2, 1))
+        F = rng.standard_normal((m, n, n))
+        groups.append(g)
+        Fs.append(torch.tensor(F + F.transpose(0, 2, 1)))
+    for active in (None, [np.array([True, False, True]), np.array([False]), np.array([False, True, True, False])]):
+        out = jb._diag_all(groups, Fs, active)
+        for k, (g, F) in enumerate(zip(groups, Fs)):
+            eps, C = out[k]
+            for i in range(F.shape[0]):
+                if active is not None and not active[k][i]:
+                    assert torch.all(eps[i] == 0) and torch.equal(C[i], g.X[i])
+                    continue
+                A = g.X[i].T @ F[i] @ g.X[i]
+                e_ref, _ = torch.linalg.eigh(A)
+                torch.testing.assert_close(eps[i], e_ref, rtol=0, atol=1e-12)
+                # C^T F C = diag(eps) and C^T S C = 1 with S = X^-2
+                torch.testing.assert_close(C[i].T @ F[i] @ C[i], torch.diag(eps[i]), rtol=0, atol=1e-10)
+                Xi = torch.linalg.inv(g.X[i])
+                torch.testing.assert_close(C[i].T @ (Xi @ Xi) @ C[i], torch.eye(F.shape[-1], dtype=F.dtype),
+                                           rtol=0, atol=1e-10)
+    assert torch.get_num_threads() == n_threads  # the caller's solver threads are left as they were
