@@ -6,7 +6,9 @@
 //            Taylor series  F_M(T_i - d) = sum_k F_{M+k}(T_i) d^k / k!
 //            (|d| <= 1/32; 8 terms in FP64 (truncation ~2e-17 relative),
 //            5 terms in FP32), then the stable downward recursion
-//            F_{m-1} = (2T F_m + e^{-T}) / (2m-1).
+//            F_{m-1} = (2T F_m + e^{-T}) / (2m-1), with e^{-T} from the
+//            same row for M <= 2 (see kBoysDerivMaxM) and from a table of
+//            e^{-T_i} above.
 //   T >= 36: F_0 = sqrt(pi/T)/2 (erf(6) = 1 to 2e-17), then upward
 //            recursion F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T), well
 //            conditioned for T > m.
@@ -90,13 +92,38 @@ __device__ __forceinline__ void boys_row(const double* __restrict__ r, double (&
 }
 __device__ __forceinline__ void boys_row(const float* __restrict__ r, float (&v)[8]) { ldg32B(r, v); }
 
-// Writes F_0 .. F_M at T into F[0..M] from the aligned table `tabA`.
-// e^{-t} comes from the tabulated e^{-T_i} for every t (0 beyond the end of
-// its grid), so only the few operations that differ between the Taylor
-// branch (t < kBoysTMax) and the asymptotic branch diverge inside a warp.
+// Orders up to this take e^{-t} of the Taylor branch from the table row
+// itself: the row of order M holds F_{M+k}(T_i)/k!, so the derivative of the
+// Taylor polynomial is F_{M+1}(t) (one term shorter) and
+//   e^{-t} = (2M+1) F_M(t) - 2t F_{M+1}(t)
+// (the upward recursion solved for e^{-t}).  The cancellation at large t
+// costs nothing: the error it leaves in e^{-t} is a rounding of F_M, which the
+// downward recursion divides by 2t.  Measured against 40-digit values over
+// [0, 36): 4.4e-16 (M = 1) and 8.7e-16 (M = 2) largest relative error of
+// F_0..F_M, against 2.2e-15 at M = 6 (the shorter F_{M+1} series), so the
+// higher orders keep the tabulated e^{-T_i}.  Dropping that load from the
+// Taylor lanes matters because a scattered per-lane load costs one L1
+// wavefront per lane whatever its width: the table gathers bound the low-L
+// J/K kernels.
+constexpr int kBoysDerivMaxM = 2;
+
+// The asymptotic branch needs e^{-t} only while it is above 2^-60 of
+// (2m+1) F_m(t) for some m < M: up to t = 44, 48, 51, 54, 56, 59, 61, 64 for
+// M = 1..8 (81 at M = 16); beyond 42 + 3M its term is dropped (and not loaded).
+__host__ __device__ constexpr int boys_exp_tcut(int M) { return 42 + 3 * M; }
+
+// Writes F_0 .. F_M at T into F[0..M] from the aligned table `tabA`.  For
+// M <= kBoysDerivMaxM every lane issues one gather at most: the table row
+// (Taylor branch) or the e^{-T_i} value (asymptotic branch below
+// boys_exp_tcut).
 template <typename T, int M>
 __device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F)[M + 1]) {
   constexpr int KT = BoysConst<T>::kTaylor;
+  constexpr bool kDeriv = M > 0 && M <= kBoysDerivMaxM;
+  // FP32 rows carry 8 values of which F_M's series uses KT = 5; with the
+  // derivative it takes one more (6 terms for F_M, 5 for F_{M+1}).  FP64 uses
+  // all 8 (8 and 7).
+  constexpr int KP = (kDeriv && KT < kBoysARow) ? KT + 1 : KT;
   const T tc = t < T(kBoysExpTEnd) ? t : T(kBoysExpTEnd);
   // i = round(16 tc) without conversion instructions: adding 1.5 * 2^52
   // (2^23 in FP32) to 0 <= x < 2^22 leaves round-to-nearest(x) in the low
@@ -104,23 +131,43 @@ __device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F
   const T xr = tc * T(kBoysGridInv) + RoundMagic<T>::value;
   const int i = RoundMagic<T>::low(xr);
   const T d = (xr - RoundMagic<T>::value) * T(1.0 / kBoysGridInv) - tc;  // T_i - t, |d| <= 1/32
-  T e = T(0);
-  if constexpr (M > 0) {
-    // e^{-t} = e^{-T_i} e^{d}, e^d by Horner over the coefficients 1/k!
+  const bool taylor = t < T(kBoysTMax);
+  T eT = T(0);
+  if constexpr (kDeriv) {
+    if (!taylor && t < T(boys_exp_tcut(M))) eT = __ldg(tabA + kBoysExpOff + i);
+  } else if constexpr (M > 0) {
+    eT = __ldg(tabA + kBoysExpOff + i);
+  }
+  // e^{-t} = e^{-T_i} e^{d}, e^d by Horner over the coefficients 1/k!
+  auto exp_d = [&]() {
     T ed = T(inv_factorial(KT - 1));
 #pragma unroll
     for (int k = KT - 2; k >= 0; --k) ed = ed * d + T(inv_factorial(k));
-    e = __ldg(tabA + kBoysExpOff + i) * ed;
-  }
-  if (t < T(kBoysTMax)) {
+    return eT * ed;
+  };
+  T e = T(0);
+  if constexpr (M > 0 && !kDeriv) e = exp_d();
+  if (taylor) {
     // the row holds F_{M+k}(T_i) / k!: the Taylor series in d is a Horner
     // chain of fused multiply-adds
     T v[8];
     boys_row(tabA + (M * kBoysRows + i) * kBoysARow, v);
-    T acc = v[KT - 1];
+    if constexpr (kDeriv) {
+      // value and derivative of the polynomial in one pass
+      T acc = v[KP - 1], der = T(0);
 #pragma unroll
-    for (int k = KT - 2; k >= 0; --k) acc = acc * d + v[k];
-    F[M] = acc;
+      for (int k = KP - 2; k >= 0; --k) {
+        der = der * d + acc;
+        acc = acc * d + v[k];
+      }
+      F[M] = acc;
+      e = T(2 * M + 1) * acc - (t + t) * der;
+    } else {
+      T acc = v[KT - 1];
+#pragma unroll
+      for (int k = KT - 2; k >= 0; --k) acc = acc * d + v[k];
+      F[M] = acc;
+    }
     if constexpr (M > 0) {
       const T t2 = t + t;
 #pragma unroll
@@ -130,6 +177,7 @@ __device__ __forceinline__ void boys_eval(T t, const T* __restrict__ tabA, T (&F
     const T r = boys_rsqrt(t);
     F[0] = T(0.88622692545275801364908374167057) * r;  // sqrt(pi)/2 / sqrt(t)
     if constexpr (M > 0) {
+      if constexpr (kDeriv) e = exp_d();
       const T half_inv_t = T(0.5) * (r * r);
 #pragma unroll
       for (int m = 0; m < M; ++m) F[m + 1] = (T(2 * m + 1) * F[m] - e) * half_inv_t;

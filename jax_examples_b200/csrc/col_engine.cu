@@ -179,6 +179,8 @@ __global__ void __launch_bounds__(32 * kColWarps) col_jk_kernel(const JKParams p
   for (int kk = 0; kk < task.nket; ++kk) {
     const int kidx = task.ket0 + kk;
     const ShellPair kp = prm.pairs[kidx];
+    if (prm.dmax_top != nullptr && float(bp.Q) * float(kp.Q) * (2.f * *prm.dmax_top) < prm.dens_tau)
+      continue;  // below the bound for any density block
     if (prm.dmax != nullptr) {
       const float* dm = prm.dmax;
       const int ns = prm.n_shell;

@@ -683,17 +683,19 @@ static TaskSet* find_jk_tasks(jqc_ctx* c, int mode, double mixed_tau) {
 // stream operations: no allocation, no host synchronisation except for the
 // timed form, so the untimed form can be captured into a CUDA graph.
 static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D, double* J, double* K,
-                      float* dmax, double dens_tau, cudaStream_t s, double* class_ms) {
+                      float* dmax, float* dmax_top, double dens_tau, cudaStream_t s, double* class_ms) {
   const int n = c->n_bf;
   const size_t nn = (size_t)n * n * n_dens;
   JQC_CUDA_CHECK(cudaMemsetAsync(J, 0, nn * sizeof(double), s));
   JQC_CUDA_CHECK(cudaMemsetAsync(K, 0, nn * sizeof(double), s));
   if (class_ms)
     for (int k = 0; k < 2 * kNumQuartetClasses; ++k) class_ms[k] = 0.0;
-  if (dens_tau > 0.0 && dmax != nullptr)
-    JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, dmax, s));
-  else
+  if (dens_tau > 0.0 && dmax != nullptr) {
+    JQC_CUDA_CHECK(launch_dmax(D, n_dens, n, c->n_shell, c->d_ao.ptr, c->d_l.ptr, dmax, dmax_top, s));
+  } else {
     dmax = nullptr;
+    dmax_top = nullptr;
+  }
   // Molecules flagged inactive leave the build before any class kernel runs:
   // the lists are compacted on the device.
   const bool compact = c->d_mol_active != nullptr && ts->comp_ready && ts->comp_nseg > 0;
@@ -725,6 +727,7 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
       p.n = n;
       p.n_dens = n_dens;
       p.dmax = dmax;
+      p.dmax_top = dmax_top;
       p.n_shell = c->n_shell;
       p.dens_tau = (float)dens_tau;
       p.threads = c->tune[qc].threads;
@@ -1247,16 +1250,19 @@ int jqc_grad2e_ex(jqc_ctx* c, int n_dens, const double* D, double j_scale, doubl
   JQC_REQUIRE(!(capturing && class_ms), JQC_ERR_INVALID, "jqc_grad2e_ex: timing cannot run inside a graph capture");
   JQC_REQUIRE(c->grad_tasks.valid || !capturing, JQC_ERR_NOT_READY,
               "jqc_grad2e: no gradient work list; call jqc_grad2e once before the capture");
-  JQC_REQUIRE(dens_tau <= 0.0 || !capturing || c->d_dmax.n >= (size_t)c->n_shell * c->n_shell, JQC_ERR_NOT_READY,
+  JQC_REQUIRE(dens_tau <= 0.0 || !capturing || c->d_dmax.n >= (size_t)c->n_shell * c->n_shell + 1, JQC_ERR_NOT_READY,
               "jqc_grad2e: density screening scratch not allocated; call once before the capture");
   if (!c->grad_tasks.valid) {
     rc = build_tasks(c, c->grad_tasks, JQC_PREC_FP64, 0.0, false, s, true);
     if (rc) return rc;
   }
   const float* dmax = nullptr;
+  float* dmax_top = nullptr;
   if (dens_tau > 0.0) {
-    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
-    JQC_CUDA_CHECK(launch_dmax(D, n_dens, c->n_bf, c->n_shell, c->d_ao.ptr, c->d_l.ptr, c->d_dmax.ptr, s));
+    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell + 1));
+    dmax_top = c->d_dmax.ptr + (size_t)c->n_shell * c->n_shell;
+    JQC_CUDA_CHECK(
+        launch_dmax(D, n_dens, c->n_bf, c->n_shell, c->d_ao.ptr, c->d_l.ptr, c->d_dmax.ptr, dmax_top, s));
     dmax = c->d_dmax.ptr;
   }
   const int n_pairs = (int)c->pairs.size();
@@ -1286,6 +1292,7 @@ int jqc_grad2e_ex(jqc_ctx* c, int n_dens, const double* D, double j_scale, doubl
     p.grad = grad;
     p.pair_force = c->d_pair_force.ptr;
     p.dmax = dmax;
+    p.dmax_top = dmax_top;
     p.n_shell = c->n_shell;
     p.dens_tau = (float)dens_tau;
     const int pb = qc_bra(qc), pk = qc_ket(qc);
@@ -1405,17 +1412,19 @@ static int jk_impl(jqc_ctx* c, int n_dens, const double* D, double* J, double* K
     // inside a capture nothing may be allocated or uploaded
     JQC_REQUIRE(find_jk_tasks(c, precision_mode, mixed_tau) != nullptr, JQC_ERR_NOT_READY,
                 "jqc_jk: no work list for this precision_mode/mixed_tau; call jqc_jk once before the capture");
-    JQC_REQUIRE(dens_tau <= 0.0 || c->d_dmax.n >= (size_t)c->n_shell * c->n_shell, JQC_ERR_NOT_READY,
+    JQC_REQUIRE(dens_tau <= 0.0 || c->d_dmax.n >= (size_t)c->n_shell * c->n_shell + 1, JQC_ERR_NOT_READY,
                 "jqc_jk: density screening scratch not allocated; call jqc_jk once before the capture");
   }
   rc = ensure_jk_tasks(c, precision_mode, mixed_tau, s);
   if (rc) return rc;
   float* dmax = nullptr;
+  float* dmax_top = nullptr;
   if (dens_tau > 0.0) {
-    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
+    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell + 1));
     dmax = c->d_dmax.ptr;
+    dmax_top = dmax + (size_t)c->n_shell * c->n_shell;
   }
-  return run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dens_tau, s, class_ms);
+  return run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dmax_top, dens_tau, s, class_ms);
 }
 
 // ----------------------------------------------------------- CUDA graphs
@@ -1601,9 +1610,11 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
     }
   }
   float* dmax = nullptr;
+  float* dmax_top = nullptr;
   if (dens_tau > 0.0) {
-    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell));
+    JQC_CUDA_CHECK(c->d_dmax.reserve((size_t)c->n_shell * c->n_shell + 1));
     dmax = c->d_dmax.ptr;
+    dmax_top = dmax + (size_t)c->n_shell * c->n_shell;
   }
   // per-class time of the current settings: min over two timed builds, or
   // one when a build takes long enough (> 30 ms) for one to be steady
@@ -1611,7 +1622,7 @@ int jqc_autotune(jqc_ctx* c, int n_dens, const double* D, double* J, double* K, 
   auto time_classes = [&](double* per_class) -> int {
     for (int qc = 0; qc < kNumQuartetClasses; ++qc) per_class[qc] = 1e300;
     for (int rep = 0; rep < 2; ++rep) {
-      int r = run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dens_tau, s, ms);
+      int r = run_jk_set(c, c->jk_cur, n_dens, D, J, K, dmax, dmax_top, dens_tau, s, ms);
       if (r) return r;
       double total = 0.0;
       for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
@@ -1744,7 +1755,10 @@ int jk_run_preallocated(jqc_ctx* c, int n_dens, const double* D, double* J, doub
               "with the same settings first, at a point where allocation is allowed");
   int rc = select_device(c);
   if (rc) return rc;
-  return run_jk_set(c, ts, n_dens, D, J, K, dmax_scratch, dens_tau, s, nullptr);
+  // the largest block maximum goes after the blocks when the scratch has room
+  const size_t nb = (size_t)c->n_shell * c->n_shell;
+  float* dmax_top = nb + 1 <= dmax_capacity ? dmax_scratch + nb : nullptr;
+  return run_jk_set(c, ts, n_dens, D, J, K, dmax_scratch, dmax_top, dens_tau, s, nullptr);
 }
 
 }  // namespace jqc

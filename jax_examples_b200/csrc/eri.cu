@@ -194,22 +194,45 @@ cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool 
 
 // --------------------------------------------------------------- helpers
 __global__ void dmax_kernel(const double* __restrict__ D, int n_dens, int n, int n_shell, const int* __restrict__ ao,
-                            const int* __restrict__ l, float* __restrict__ dmax) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n_shell * n_shell) return;
-  const int i = idx / n_shell, j = idx % n_shell;
-  const int ni = ncart(l[i]), nj = ncart(l[j]);
-  double m = 0.0;
-  for (int d = 0; d < n_dens; ++d)
-    for (int a = 0; a < ni; ++a)
-      for (int b = 0; b < nj; ++b) m = fmax(m, fabs(D[(size_t)d * n * n + (size_t)(ao[i] + a) * n + ao[j] + b]));
-  dmax[idx] = float(m);
+                            const int* __restrict__ l, float* __restrict__ dmax, float* __restrict__ dmax_top) {
+  const long long tot = (long long)n_shell * n_shell;
+  float top = 0.f;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < tot;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = int(idx / n_shell), j = int(idx % n_shell);
+    const int ni = ncart(l[i]), nj = ncart(l[j]);
+    double m = 0.0;
+    for (int d = 0; d < n_dens; ++d)
+      for (int a = 0; a < ni; ++a)
+        for (int b = 0; b < nj; ++b) m = fmax(m, fabs(D[(size_t)d * n * n + (size_t)(ao[i] + a) * n + ao[j] + b]));
+    dmax[idx] = float(m);
+    top = fmaxf(top, float(m));
+  }
+  if (dmax_top == nullptr) return;  // uniform over the launch
+  // block maximum, then one atomic per block: non-negative floats order as
+  // their bit patterns do
+  __shared__ float warp_top[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) top = fmaxf(top, __shfl_xor_sync(0xffffffffu, top, o));
+  if ((threadIdx.x & 31) == 0) warp_top[threadIdx.x >> 5] = top;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t = fmaxf(t, warp_top[w]);
+    if (t > 0.f) atomicMax(reinterpret_cast<int*>(dmax_top), __float_as_int(t));
+  }
 }
 
 cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
-                        cudaStream_t s) {
-  const int tot = n_shell * n_shell;
-  dmax_kernel<<<(tot + 255) / 256, 256, 0, s>>>(D, n_dens, n, n_shell, ao, l, dmax);
+                        float* dmax_top, cudaStream_t s) {
+  const long long tot = (long long)n_shell * n_shell;
+  if (dmax_top != nullptr) {
+    const cudaError_t e = cudaMemsetAsync(dmax_top, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+  }
+  if (tot == 0) return cudaSuccess;
+  const long long blocks = std::min<long long>((tot + 255) / 256, 2048);
+  dmax_kernel<<<(unsigned)blocks, 256, 0, s>>>(D, n_dens, n, n_shell, ao, l, dmax, dmax_top);
   return cudaGetLastError();
 }
 

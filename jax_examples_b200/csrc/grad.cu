@@ -136,6 +136,8 @@ __global__ void __launch_bounds__(32 * kGradWarps, 4) warp_grad_kernel(const Gra
     const double Dx = ctr[3 * kp.b], Dy = ctr[3 * kp.b + 1], Dz = ctr[3 * kp.b + 2];
     const int c0 = prm.ao[kp.a], d0 = prm.ao[kp.b];
     // density screening (warp-uniform: one quartet at a time)
+    if (prm.dmax_top != nullptr && float(bp.Q) * float(kp.Q) * gamma_bound_top(prm, *prm.dmax_top) < prm.dens_tau)
+      continue;
     if (prm.dmax != nullptr && float(bp.Q) * float(kp.Q) * gamma_bound(prm, bp.a, bp.b, kp.a, kp.b) < prm.dens_tau)
       continue;
     // Gamma for this quartet

@@ -65,6 +65,9 @@ struct GradBody {
     const int kidx = task.ket0 + (in_range ? lane : 0);
     const ShellPair kp = prm.pairs[kidx];
     bool active = in_range;
+    if (prm.dmax_top != nullptr && active &&
+        float(bp.Q) * float(kp.Q) * gamma_bound_top(prm, *prm.dmax_top) < prm.dens_tau)
+      active = false;  // below the bound for any density block: no gathers
     if (prm.dmax != nullptr && active &&
         float(bp.Q) * float(kp.Q) * gamma_bound(prm, bp.a, bp.b, kp.a, kp.b) < prm.dens_tau)
       active = false;

@@ -282,6 +282,8 @@ __global__ void __launch_bounds__(32 * kGRowWarps, grad_row_min_blocks(LA, LB, L
   for (int kk = 0; kk < task.nket; ++kk) {
     const int kidx = task.ket0 + kk;
     const ShellPair kp = prm.pairs[kidx];
+    if (prm.dmax_top != nullptr && float(bp.Q) * float(kp.Q) * gamma_bound_top(prm, *prm.dmax_top) < prm.dens_tau)
+      continue;  // warp-uniform
     if (prm.dmax != nullptr && float(bp.Q) * float(kp.Q) * gamma_bound(prm, bp.a, bp.b, kp.a, kp.b) < prm.dens_tau)
       continue;  // warp-uniform
     const double Cx = ctr[3 * kp.a], Cy = ctr[3 * kp.a + 1], Cz = ctr[3 * kp.a + 2];

@@ -90,6 +90,8 @@ struct JKBody {
     bool active = in_range;
     // a compacted packed group may hold tasks of several molecules
     if (kPacked && prm.items != nullptr && active) active = prm.mol_active[prm.shell_mol[bp.a]] != 0;
+    if (prm.dmax_top != nullptr && active && float(bp.Q) * float(kp.Q) * (2.f * *prm.dmax_top) < prm.dens_tau)
+      active = false;  // below the bound for any density block: no gathers
     if (prm.dmax != nullptr && active) {
       const float* dm = prm.dmax;
       const int ns = prm.n_shell;
@@ -182,35 +184,116 @@ struct JKBody {
         });
         atomicAdd(Jm + (size_t)(c0 + c) * n + d0 + d, 2.0 * s * acc);
       });
-      // K: four blocks, for the (c, d) of this part.
-      static_for<NCDP>([&](auto cdi_) {
-        constexpr int cdi = decltype(cdi_)::value;
-        constexpr int cd = Cfg::CD0 + cdi, c = cd / ND, d = cd % ND;
-        // K[a][d] += sum_b v D[c][b];  K[a][c] += sum_b v D[d][b]
-        static_for<NA>([&](auto a_) {
-          constexpr int a = decltype(a_)::value;
-          double kad = 0.0, kac = 0.0;
-          static_for<NB>([&](auto b_) {
-            constexpr int b = decltype(b_)::value;
-            const double v = double(out[a * NB + b][cdi]);
-            kad += v * __ldg(Dm + (size_t)(c0 + c) * n + b0 + b);
-            kac += v * __ldg(Dm + (size_t)(d0 + d) * n + b0 + b);
-          });
-          atomicAdd(Km + (size_t)(a0 + a) * n + d0 + d, s * kad);
-          atomicAdd(Km + (size_t)(a0 + a) * n + c0 + c, s * kac);
+      // K: four blocks, for the (c, d) of this part.  Every D element and
+      // every K target is touched once per quartet: K[a][d] sums over b and
+      // c in registers before its one atomic (not one atomic per (c, d)
+      // component), and each D element is loaded once.  D is symmetric, so
+      // its elements are read as D[b][c] rather than D[c][b]: the row is the
+      // bra's (the same for the lanes of a task) and the lanes' kets spread
+      // over the columns of one row, a few cache lines, not one line a lane.
+      constexpr int NC = Cfg::NC, CD0 = Cfg::CD0;
+      auto in_part = [](int c, int d) { return c * ND + d >= CD0 && c * ND + d < CD0 + NCDP; };
+      auto has_c = [&](int c) {
+        bool r = false;
+        for (int d = 0; d < ND; ++d) r = r || in_part(c, d);
+        return r;
+      };
+      auto has_d = [&](int d) {
+        bool r = false;
+        for (int c = 0; c < NC; ++c) r = r || in_part(c, d);
+        return r;
+      };
+      // K[a][d] += sum_{b,c} v D[c][b];  K[a][c] += sum_{b,d} v D[d][b]
+      double dbc[NB][NC], dbd[NB][ND];
+      static_for<NB>([&](auto b_) {
+        constexpr int b = decltype(b_)::value;
+        static_for<NC>([&](auto c_) {
+          constexpr int c = decltype(c_)::value;
+          if constexpr (has_c(c)) dbc[b][c] = __ldg(Dm + (size_t)(b0 + b) * n + c0 + c);
         });
-        // K[b][d] += sum_a v D[c][a];  K[b][c] += sum_a v D[d][a]
-        static_for<NB>([&](auto b_) {
-          constexpr int b = decltype(b_)::value;
-          double kbd = 0.0, kbc = 0.0;
-          static_for<NA>([&](auto a_) {
-            constexpr int a = decltype(a_)::value;
-            const double v = double(out[a * NB + b][cdi]);
-            kbd += v * __ldg(Dm + (size_t)(c0 + c) * n + a0 + a);
-            kbc += v * __ldg(Dm + (size_t)(d0 + d) * n + a0 + a);
-          });
-          atomicAdd(Km + (size_t)(b0 + b) * n + d0 + d, s * kbd);
-          atomicAdd(Km + (size_t)(b0 + b) * n + c0 + c, s * kbc);
+        static_for<ND>([&](auto d_) {
+          constexpr int d = decltype(d_)::value;
+          if constexpr (has_d(d)) dbd[b][d] = __ldg(Dm + (size_t)(b0 + b) * n + d0 + d);
+        });
+      });
+      static_for<NA>([&](auto a_) {
+        constexpr int a = decltype(a_)::value;
+        static_for<ND>([&](auto d_) {
+          constexpr int d = decltype(d_)::value;
+          if constexpr (has_d(d)) {
+            double acc = 0.0;
+            static_for<NB>([&](auto b_) {
+              constexpr int b = decltype(b_)::value;
+              static_for<NC>([&](auto c_) {
+                constexpr int c = decltype(c_)::value;
+                if constexpr (in_part(c, d)) acc += double(out[a * NB + b][c * ND + d - CD0]) * dbc[b][c];
+              });
+            });
+            atomicAdd(Km + (size_t)(a0 + a) * n + d0 + d, s * acc);
+          }
+        });
+        static_for<NC>([&](auto c_) {
+          constexpr int c = decltype(c_)::value;
+          if constexpr (has_c(c)) {
+            double acc = 0.0;
+            static_for<NB>([&](auto b_) {
+              constexpr int b = decltype(b_)::value;
+              static_for<ND>([&](auto d_) {
+                constexpr int d = decltype(d_)::value;
+                if constexpr (in_part(c, d)) acc += double(out[a * NB + b][c * ND + d - CD0]) * dbd[b][d];
+              });
+            });
+            atomicAdd(Km + (size_t)(a0 + a) * n + c0 + c, s * acc);
+          }
+        });
+      });
+      // K[b][d] += sum_{a,c} v D[c][a];  K[b][c] += sum_{a,d} v D[d][a]
+      // (the bra's second shell has the fewer functions: its sums stay in
+      // registers while the D[a][.] elements stream past)
+      double kbd[NB][ND], kbc[NB][NC];
+      static_for<NB>([&](auto b_) {
+        constexpr int b = decltype(b_)::value;
+        static_for<ND>([&](auto d_) { kbd[b][decltype(d_)::value] = 0.0; });
+        static_for<NC>([&](auto c_) { kbc[b][decltype(c_)::value] = 0.0; });
+      });
+      static_for<NA>([&](auto a_) {
+        constexpr int a = decltype(a_)::value;
+        static_for<NC>([&](auto c_) {
+          constexpr int c = decltype(c_)::value;
+          if constexpr (has_c(c)) {
+            const double x = __ldg(Dm + (size_t)(a0 + a) * n + c0 + c);
+            static_for<NB>([&](auto b_) {
+              constexpr int b = decltype(b_)::value;
+              static_for<ND>([&](auto d_) {
+                constexpr int d = decltype(d_)::value;
+                if constexpr (in_part(c, d)) kbd[b][d] += double(out[a * NB + b][c * ND + d - CD0]) * x;
+              });
+            });
+          }
+        });
+        static_for<ND>([&](auto d_) {
+          constexpr int d = decltype(d_)::value;
+          if constexpr (has_d(d)) {
+            const double x = __ldg(Dm + (size_t)(a0 + a) * n + d0 + d);
+            static_for<NB>([&](auto b_) {
+              constexpr int b = decltype(b_)::value;
+              static_for<NC>([&](auto c_) {
+                constexpr int c = decltype(c_)::value;
+                if constexpr (in_part(c, d)) kbc[b][c] += double(out[a * NB + b][c * ND + d - CD0]) * x;
+              });
+            });
+          }
+        });
+      });
+      static_for<NB>([&](auto b_) {
+        constexpr int b = decltype(b_)::value;
+        static_for<ND>([&](auto d_) {
+          constexpr int d = decltype(d_)::value;
+          if constexpr (has_d(d)) atomicAdd(Km + (size_t)(b0 + b) * n + d0 + d, s * kbd[b][d]);
+        });
+        static_for<NC>([&](auto c_) {
+          constexpr int c = decltype(c_)::value;
+          if constexpr (has_c(c)) atomicAdd(Km + (size_t)(b0 + b) * n + c0 + c, s * kbc[b][c]);
         });
       });
     }

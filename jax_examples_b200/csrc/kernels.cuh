@@ -35,6 +35,10 @@ struct JKParams {
   const float* dmax;       // n_shell x n_shell max |D| per shell block, or null
   int n_shell;
   float dens_tau;
+  // The largest entry of dmax (one float), or null.  A lane whose bound
+  // Q_ab Q_cd 2 max(dmax) is below dens_tau fails the per-block test too, so
+  // it leaves before the six block-maximum gathers.
+  const float* dmax_top = nullptr;
   int threads = 128;       // threads per block (64, 128, 256)
   int persistent = 0;      // 1: grid capped at the resident blocks, warps stride over tasks
   int engine = kEngineReg; // JKEngine
@@ -108,8 +112,10 @@ cudaError_t launch_schwarz(int pc, const SchwarzParams& p, cudaStream_t s);
 cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s);
 // tabA: the aligned per-order Boys table of the output type.
 cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool fp32, const void* tabA, cudaStream_t s);
+// dmax[i * n_shell + j] = max |D^s| over the (i, j) shell block and the
+// densities; with dmax_top non-null also the largest of them into *dmax_top.
 cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
-                        cudaStream_t s);
+                        float* dmax_top, cudaStream_t s);
 cudaError_t launch_symmetrize(double* M, int count, int n, cudaStream_t s);
 // Writes, for every segment, the indices of the work items that hold a task
 // of an active molecule (mol_active[shell_mol[shell a of the bra pair]] != 0)
@@ -154,6 +160,7 @@ struct GradParams {
   // folds them into grad (n_atom x 3 would take every atomic of the launch).
   double* pair_force = nullptr;
   const float* dmax = nullptr;  // n_shell x n_shell max |D^s| per shell block, or null
+  const float* dmax_top = nullptr;  // the largest entry of dmax, or null
   int n_shell = 0;
   float dens_tau = 0.f;   // skip quartets whose Gamma bound x Q_ab Q_cd is below this
   int sides = 1;          // register kernels: 2 = bra and ket forces in separate block parts
@@ -172,6 +179,14 @@ __device__ __forceinline__ float gamma_bound(const GradParams& p, int a, int b, 
   const float nd = float(p.n_dens);
   return float(p.jscale) * nd * nd * m[a * ns + b] * m[c * ns + d] +
          0.5f * float(p.kscale) * nd * (m[a * ns + c] * m[b * ns + d] + m[a * ns + d] * m[b * ns + c]);
+}
+
+// gamma_bound with every block maximum replaced by their largest, g: the same
+// expression tree, so in floating point too it is never below gamma_bound of
+// any quartet, and a quartet it screens out is screened out by gamma_bound.
+__device__ __forceinline__ float gamma_bound_top(const GradParams& p, float g) {
+  const float nd = float(p.n_dens);
+  return float(p.jscale) * nd * nd * g * g + 0.5f * float(p.kscale) * nd * (g * g + g * g);
 }
 
 struct Grad1Params {

@@ -15,9 +15,10 @@ the precision policy of the mixed path:
   ``rebuild_every`` builds of the mixed phase (itself screened at ``mixed_full_dens_tau``, 1e-9:
   8.3 -> 5.6 ms on (H2O)16 with the same iterations and final error).  In
   this phase the incremental builds screen at
-  ``mixed_dens_tau`` (1e-8: the early Fock matrices only steer the next
-  density; 3e-8 and a threshold that follows the DIIS error upward already
-  cost more iterations than they save).  When the SCF error
+  ``mixed_dens_tau``, raised to ``mixed_dens_rel`` times the last SCF error
+  while that is larger (the early Fock matrices only steer the next density;
+  a factor of 1e-6 saves 4-10% of the Fock time, 1e-5 and more cost erratic
+  extra iterations).  When the SCF error
   drops below ``fp64_switch`` the builder switches to FP64 with a full
   rebuild (screened at ``fp64_switch_dens_tau``, unscreened by default; it
   drops the errors of the mixed phase) and then incremental
@@ -111,6 +112,8 @@ class FockBuilder:
         self.rebuild_every = rebuild_every
         self.dens_tau = dens_tau
         self.mixed_dens_tau = float(getattr(config, "mixed_dens_tau", 1e-8))
+        self.mixed_dens_rel = float(getattr(config, "mixed_dens_rel", 0.0))  # 0: fixed threshold
+        self._last_err = None  # max|DIIS error| of the last iteration
         self.tail_dens_tau = float(getattr(config, "fp64_tail_dens_tau", dens_tau))
         self.mixed_full_dens_tau = float(getattr(config, "mixed_full_dens_tau", 0.0))
         self.switch_dens_tau = float(getattr(config, "fp64_switch_dens_tau", 0.0))
@@ -147,6 +150,8 @@ class FockBuilder:
             dD = D - self._prev[0]
             if prec == "mixed":
                 tau = max(self.mixed_dens_tau, self.dens_tau)
+                if self.mixed_dens_rel > 0.0 and self._last_err is not None:
+                    tau = max(tau, self.mixed_dens_rel * self._last_err)
             elif self.precision == "mixed":
                 tau = max(self.tail_dens_tau, self.dens_tau)  # FP64 tail of the mixed policy
             else:
@@ -190,6 +195,7 @@ class FockBuilder:
     def observe(self, err_max: float) -> bool:
         """Called once per SCF iteration with max|DIIS error|; True when this
         call switched the builder from the mixed phase to FP64."""
+        self._last_err = float(err_max)
         if self.phase == "mixed" and err_max < self.fp64_switch:
             self.phase = "fp64"
             self.switched = True
