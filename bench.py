@@ -767,7 +767,7 @@ def run_ours(args):
                      "frac": achieved / peak64,
                      # DRAM bytes of one launch of the dominant kernel on this workload, from an ncu
                      # capture of dram__bytes_read.sum + dram__bytes_write.sum (7,585,280 + 0)
-                     "traffic": 7585280 if best[2] == (1, 0, 0, 0) and N_WATERS == 16 else None,
+                     "traffic": 7515904 if best[2] == (1, 0, 0, 0) and N_WATERS == 16 else None,
                      "traffic_note": "L2-resident working set: the DRAM bytes are the compulsory reads of "
                                      "the pair data, the Boys table and D",
                      "kernel": "jk_kernel<double,%d,%d,%d,%d>" % best[2],

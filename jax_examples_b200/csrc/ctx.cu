@@ -183,8 +183,9 @@ struct TaskSet {
   long long n_prim_quartets = 0;
   long long class_quartets[2][kNumQuartetClasses] = {};
   long long class_prims[2][kNumQuartetClasses] = {};
-  // molecule compaction (batch contexts): one segment per non-empty list,
-  // the surviving item indices of segment k at d_items + comp_item_off[k]
+  // device-side compaction of the lists (inactive molecules of a batch,
+  // density screening): one segment per non-empty list, the surviving item
+  // indices of segment k at d_items + comp_item_off[k]
   bool comp_ready = false;
   int comp_nseg = 0;
   long long comp_total = 0;
@@ -194,6 +195,7 @@ struct TaskSet {
   DevBuf<int> d_counts;
   DevBuf<CompactSeg> d_segs;
   DevBuf<long long> d_seg_start;
+  DevBuf<float> d_item_q;  // per item bound of the density test, segment by segment
 };
 
 // Pairs of one (class, primitive-pair count, molecule), Q descending.
@@ -565,12 +567,15 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
   ts.mixed_tau = mixed_tau;
   ts.full = full;
   ts.valid = true;
-  // Batch contexts: segments for the device-side molecule compaction of the
-  // lists (used while jqc_set_molecule_activity is set).
+  // Segments for the device-side compaction of the lists (used while
+  // jqc_set_molecule_activity is set and by density-screened builds), with
+  // each item's largest float(Q_bra) float(Q_ket): the kernels' density bound
+  // is that times 2 max|D block|, computed with the same operations.
   ts.comp_ready = false;
-  if (c->n_mol > 1 && !full && !grad) {
+  if (!full && !grad) {
     std::vector<CompactSeg> segs;
     std::vector<long long> starts;
+    std::vector<float> item_q;
     long long tot = 0;
     int nseg = 0;
     for (int prec = 0; prec < 2; ++prec)
@@ -581,13 +586,29 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
         ts.comp_seg_of[prec][qc] = nseg;
         ts.comp_item_off[nseg] = tot;
         starts.push_back(tot);
-        segs.push_back(CompactSeg{nullptr, nullptr, items, nullptr, nullptr});
+        segs.push_back(CompactSeg{nullptr, nullptr, items, nullptr, nullptr, nullptr});
+        const Task* lt = ts.h.data() + ts.off[prec][qc];
+        auto task_q = [&](const Task& t) {
+          return float(c->pairs[t.bra].Q) * float(c->pairs[t.ket0].Q);  // ket runs: Q-descending
+        };
+        for (int it = 0; it < items; ++it) {
+          float q = 0.f;
+          if (ts.gcnt[prec][qc] > 0) {
+            const int* gb = ts.gh.data() + ts.goff[prec][qc];
+            for (int t = gb[it]; t < gb[it + 1]; ++t) q = std::max(q, task_q(lt[t]));
+          } else {
+            q = task_q(lt[it]);
+          }
+          item_q.push_back(q);
+        }
         tot += items;
         ++nseg;
       }
     starts.push_back(tot);
     JQC_CUDA_CHECK(ts.d_items.reserve((size_t)std::max<long long>(tot, 1)));
     JQC_CUDA_CHECK(ts.d_counts.reserve((size_t)std::max(nseg, 1)));
+    if (item_q.empty()) item_q.push_back(0.f);
+    JQC_CUDA_CHECK(ts.d_item_q.upload(item_q, s));
     int k = 0;
     for (int prec = 0; prec < 2; ++prec)
       for (int qc = 0; qc < kNumQuartetClasses; ++qc) {
@@ -597,6 +618,7 @@ static int build_tasks(jqc_ctx* c, TaskSet& ts, int mode, double mixed_tau, bool
         sg.groups = ts.gcnt[prec][qc] > 0 ? ts.gd.ptr + ts.goff[prec][qc] : nullptr;
         sg.out = ts.d_items.ptr + ts.comp_item_off[k];
         sg.count = ts.d_counts.ptr + k;
+        sg.item_q = ts.d_item_q.ptr + ts.comp_item_off[k];
         ++k;
       }
     JQC_CUDA_CHECK(ts.d_segs.upload(segs, s));
@@ -696,13 +718,15 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
     dmax = nullptr;
     dmax_top = nullptr;
   }
-  // Molecules flagged inactive leave the build before any class kernel runs:
-  // the lists are compacted on the device.
-  const bool compact = c->d_mol_active != nullptr && ts->comp_ready && ts->comp_nseg > 0;
+  // Molecules flagged inactive, and work items whose every lane is below the
+  // density bound, leave the build before any class kernel runs: the lists
+  // are compacted on the device.
+  const bool compact = (c->d_mol_active != nullptr || dmax_top != nullptr) && ts->comp_ready && ts->comp_nseg > 0;
   if (compact) {
     JQC_CUDA_CHECK(cudaMemsetAsync(ts->d_counts.ptr, 0, (size_t)ts->comp_nseg * sizeof(int), s));
     JQC_CUDA_CHECK(launch_compact(ts->d_segs.ptr, ts->d_seg_start.ptr, ts->comp_nseg, ts->comp_total,
-                                  c->d_pairs.ptr, c->d_shell_mol.ptr, c->d_mol_active, s));
+                                  c->d_pairs.ptr, c->d_shell_mol.ptr, c->d_mol_active, dmax_top,
+                                  (float)dens_tau, s));
   }
   if (!class_ms) {
     JQC_CUDA_CHECK(cudaEventRecord(c->ev_fork, s));
@@ -741,8 +765,10 @@ static int run_jk_set(jqc_ctx* c, const TaskSet* ts, int n_dens, const double* D
         const int sg = ts->comp_seg_of[prec][qc];
         p.items = ts->d_items.ptr + ts->comp_item_off[sg];
         p.n_items = ts->d_counts.ptr + sg;
-        p.shell_mol = c->d_shell_mol.ptr;
-        p.mol_active = c->d_mol_active;
+        if (c->d_mol_active != nullptr) {
+          p.shell_mol = c->d_shell_mol.ptr;
+          p.mol_active = c->d_mol_active;
+        }
       }
       if (class_ms) {
         JQC_CUDA_CHECK(cudaEventRecord(c->ev_t0, s));

@@ -245,7 +245,10 @@ __global__ void __launch_bounds__(256) compact_kernel(const CompactSeg* __restri
                                                       const long long* __restrict__ seg_start, int n_segs,
                                                       long long total, const ShellPair* __restrict__ pairs,
                                                       const int* __restrict__ shell_mol,
-                                                      const int* __restrict__ mol_active) {
+                                                      const int* __restrict__ mol_active,
+                                                      const float* __restrict__ dmax_top, float dens_tau) {
+  // 2 x the largest density block maximum: the kernels' bound, same operands
+  const float top2 = dmax_top != nullptr ? 2.f * *dmax_top : 0.f;
   const int lane = threadIdx.x & 31;
   const long long step = (long long)gridDim.x * blockDim.x;
   for (long long base = (long long)blockIdx.x * blockDim.x; base < total; base += step) {
@@ -264,11 +267,16 @@ __global__ void __launch_bounds__(256) compact_kernel(const CompactSeg* __restri
       seg = lo;
       item = int(g - seg_start[seg]);
       const CompactSeg S = segs[seg];
-      if (S.groups != nullptr) {
-        for (int t = S.groups[item]; t < S.groups[item + 1] && !act; ++t)
-          act = mol_active[shell_mol[pairs[S.tasks[t].bra].a]] != 0;
-      } else {
-        act = mol_active[shell_mol[pairs[S.tasks[item].bra].a]] != 0;
+      act = true;
+      if (dmax_top != nullptr) act = !(S.item_q[item] * top2 < dens_tau);
+      if (act && mol_active != nullptr) {
+        act = false;
+        if (S.groups != nullptr) {
+          for (int t = S.groups[item]; t < S.groups[item + 1] && !act; ++t)
+            act = mol_active[shell_mol[pairs[S.tasks[t].bra].a]] != 0;
+        } else {
+          act = mol_active[shell_mol[pairs[S.tasks[item].bra].a]] != 0;
+        }
       }
     }
     const unsigned same = __match_any_sync(0xffffffffu, act ? seg : -1);
@@ -284,7 +292,8 @@ __global__ void __launch_bounds__(256) compact_kernel(const CompactSeg* __restri
 }
 
 cudaError_t launch_compact(const CompactSeg* segs, const long long* seg_start, int n_segs, long long total_items,
-                           const ShellPair* pairs, const int* shell_mol, const int* mol_active, cudaStream_t s) {
+                           const ShellPair* pairs, const int* shell_mol, const int* mol_active,
+                           const float* dmax_top, float dens_tau, cudaStream_t s) {
   if (total_items == 0 || n_segs == 0) return cudaSuccess;
   int dev = 0, sms = 148;
   cudaError_t e = cudaGetDevice(&dev);
@@ -292,7 +301,8 @@ cudaError_t launch_compact(const CompactSeg* segs, const long long* seg_start, i
   if (e != cudaSuccess) return e;
   const long long want = (total_items + 255) / 256;
   const int blocks = (int)std::min<long long>(want, (long long)sms * 8);
-  compact_kernel<<<blocks, 256, 0, s>>>(segs, seg_start, n_segs, total_items, pairs, shell_mol, mol_active);
+  compact_kernel<<<blocks, 256, 0, s>>>(segs, seg_start, n_segs, total_items, pairs, shell_mol, mol_active,
+                                        dmax_top, dens_tau);
   return cudaGetLastError();
 }
 

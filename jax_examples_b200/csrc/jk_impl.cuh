@@ -89,7 +89,7 @@ struct JKBody {
     const ShellPair kp = prm.pairs[kidx];
     bool active = in_range;
     // a compacted packed group may hold tasks of several molecules
-    if (kPacked && prm.items != nullptr && active) active = prm.mol_active[prm.shell_mol[bp.a]] != 0;
+    if (kPacked && prm.mol_active != nullptr && active) active = prm.mol_active[prm.shell_mol[bp.a]] != 0;
     if (prm.dmax_top != nullptr && active && float(bp.Q) * float(kp.Q) * (2.f * *prm.dmax_top) < prm.dens_tau)
       active = false;  // below the bound for any density block: no gathers
     if (prm.dmax != nullptr && active) {

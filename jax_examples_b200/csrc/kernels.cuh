@@ -68,6 +68,9 @@ struct CompactSeg {
   int n_items;
   int* out;
   int* count;
+  // per item the largest float(Q_bra) * float(Q_ket) of its tasks (the ket
+  // runs are Q-descending: their first pair)
+  const float* item_q;
 };
 
 constexpr int kMaxJKThreads = 256;
@@ -117,12 +120,16 @@ cudaError_t launch_boys(const double* T, long long n, int mmax, void* out, bool 
 cudaError_t launch_dmax(const double* D, int n_dens, int n, int n_shell, const int* ao, const int* l, float* dmax,
                         float* dmax_top, cudaStream_t s);
 cudaError_t launch_symmetrize(double* M, int count, int n, cudaStream_t s);
-// Writes, for every segment, the indices of the work items that hold a task
-// of an active molecule (mol_active[shell_mol[shell a of the bra pair]] != 0)
-// and their count (the counts must be zero on entry).  seg_start: n_segs + 1
-// prefix sums of the segments' item counts.
+// Writes, for every segment, the indices of the work items that survive into
+// segs[k].out and their count into *segs[k].count (the counts must be zero on
+// entry).  An item survives when (with mol_active) one of its tasks belongs to
+// an active molecule (mol_active[shell_mol[shell a of the bra pair]] != 0) and
+// (with dmax_top) item_q * 2 * (*dmax_top) is not below dens_tau: the class
+// kernels' first density test, so every lane of a dropped item would have
+// left at that test.  seg_start: n_segs + 1 prefix sums of the item counts.
 cudaError_t launch_compact(const CompactSeg* segs, const long long* seg_start, int n_segs, long long total_items,
-                           const ShellPair* pairs, const int* shell_mol, const int* mol_active, cudaStream_t s);
+                           const ShellPair* pairs, const int* shell_mol, const int* mol_active,
+                           const float* dmax_top, float dens_tau, cudaStream_t s);
 
 // Class tables: angular momenta of pair class pc.
 __host__ __device__ constexpr int pc_la(int pc) { return pc == 0 ? 0 : pc <= 2 ? 1 : 2; }
