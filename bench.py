@@ -693,35 +693,44 @@ def run_ours(args):
         for prec, tau in (("mixed", 0.0), ("mixed", 1e-8), ("fp64", 1e-11)):
             eng.jk(D, precision=prec, mixed_tau=chosen_tau, dens_tau=tau)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        # plain: a full FP64 build every iteration (the reference's Fock build)
-        r64 = run_scf(mol, ints, CalcConfig(scf_conv=1e-8, incremental=False))
-        torch.cuda.synchronize()
-        t64 = time.perf_counter() - t0
+        # plain: a full FP64 build every iteration (the reference's Fock build).
+        # The two SCFs run alternately, twice each, and each keeps its faster
+        # run, so a clock or power-cap change during the leg hits both sides.
         cfg = CalcConfig(scf_conv=1e-8, precision="mixed", incremental=True)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rmx = run_scf(mol, ints, cfg)
-        torch.cuda.synchronize()
-        tmx = time.perf_counter() - t0
+        r64 = rmx = None
+        t64 = tmx = float("inf")
+        for _ in range(2):
+            t0 = time.perf_counter()
+            r = run_scf(mol, ints, CalcConfig(scf_conv=1e-8, incremental=False))
+            torch.cuda.synchronize()
+            t64 = min(t64, time.perf_counter() - t0)
+            if r64 is None or r.precision["jk_seconds"] < r64.precision["jk_seconds"]:
+                r64 = r
+            t0 = time.perf_counter()
+            r = run_scf(mol, ints, cfg)
+            torch.cuda.synchronize()
+            tmx = min(tmx, time.perf_counter() - t0)
+            if rmx is None or r.precision["jk_seconds"] < rmx.precision["jk_seconds"]:
+                rmx = r
         from jax_examples_b200.grad import rhf_gradient
 
         rhf_gradient(mol, r64, engine=eng)  # warm-up (builds the gradient work list)
+        rhf_gradient(mol, rmx, engine=eng, dens_tau=CHOSEN_GRAD_TAU)
         torch.cuda.synchronize()
         ge0 = torch.cuda.Event(enable_timing=True)
         ge1 = torch.cuda.Event(enable_timing=True)
-        ge0.record()
-        g64 = rhf_gradient(mol, r64, engine=eng)
-        ge1.record()
-        torch.cuda.synchronize()
-        tgrad = ge0.elapsed_time(ge1) * 1e-3
-        rhf_gradient(mol, rmx, engine=eng, dens_tau=CHOSEN_GRAD_TAU)  # warm-up
-        torch.cuda.synchronize()
-        ge0.record()
-        gmx = rhf_gradient(mol, rmx, engine=eng, dens_tau=CHOSEN_GRAD_TAU)
-        ge1.record()
-        torch.cuda.synchronize()
-        tgrad_mx = ge0.elapsed_time(ge1) * 1e-3
+        tgrad = tgrad_mx = float("inf")
+        for _ in range(2):  # alternately, the faster of two each
+            ge0.record()
+            g64 = rhf_gradient(mol, r64, engine=eng)
+            ge1.record()
+            torch.cuda.synchronize()
+            tgrad = min(tgrad, ge0.elapsed_time(ge1) * 1e-3)
+            ge0.record()
+            gmx = rhf_gradient(mol, rmx, engine=eng, dens_tau=CHOSEN_GRAD_TAU)
+            ge1.record()
+            torch.cuda.synchronize()
+            tgrad_mx = min(tgrad_mx, ge0.elapsed_time(ge1) * 1e-3)
         plain_total = r64.precision["jk_seconds"] + tgrad
         chosen_total = rmx.precision["jk_seconds"] + tgrad_mx
         fg = {"mixed_work_list_build_s": round(t_wl, 4),

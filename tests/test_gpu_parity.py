@@ -165,6 +165,67 @@ def test_jk_cluster_vs_oracle_direct():
     assert np.max(np.abs(K3.cpu().numpy() - Kr)) < 1e-7
 
 
+def _screen_keep(pk, Q, D, tau=None):
+    """The density-screening rule of the J/K kernels, restated in NumPy: a
+    canonical quartet (ij|kl) is kept unless float(Q_ij) float(Q_kl) m < tau
+    in FP32, m = max(2 d_ij, 2 d_kl, d_ik, d_il, d_jk, d_jl) over the FP32
+    block maxima d of |D|.  Without tau, picks one in the middle of the
+    widest relative gap between the bounds of the middle half of the quartets
+    (so no bound sits within 0.1% of it) and returns it too."""
+    off = pk.offsets
+    ns = pk.n_shell
+    dm = np.zeros((ns, ns), dtype=np.float32)
+    for a in range(ns):
+        for b in range(ns):
+            dm[a, b] = np.float32(np.abs(D[off[a]:off[a + 1], off[b]:off[b + 1]]).max())
+    qs = oracle.canonical_quartets(ns)
+    i, j, k, l = qs.T
+    two = np.float32(2.0)
+    m = np.maximum.reduce([two * dm[i, j], two * dm[k, l], dm[i, k], dm[i, l], dm[j, k], dm[j, l]])
+    Qf = Q.astype(np.float32)
+    x = (Qf[i, j] * Qf[k, l]) * m
+    if tau is None:
+        v = np.unique(x[x > 0])
+        lo, hi = len(v) // 4, 3 * len(v) // 4
+        r = v[lo + 1:hi] / v[lo:hi - 1]
+        g = int(np.argmax(r)) + lo
+        assert v[g + 1] / v[g] > 1.001
+        tau = float(np.sqrt(float(v[g]) * float(v[g + 1])))
+    keep = ~(x < np.float32(tau))
+    return qs, keep, tau
+
+
+def test_density_screened_jk_vs_oracle_same_rule():
+    """Density screening (block maxima, the bound against their largest, and
+    the device-side compaction of work items that all fail it) drops exactly
+    the quartets the rule drops: the oracle digesting the quartets the rule
+    keeps matches the screened build at 1e-10, with a threshold that drops
+    about half of them."""
+    mol = pb.water_cluster(3, seed=1)
+    bs = pb.build_basis_set(mol, "6-31g*")
+    pk = oracle.Packed(bs)
+    rng = np.random.default_rng(11)
+    n = bs.n_basis
+    # density blocks spanning many orders of magnitude: decay with the
+    # distance between the functions' centres
+    ctr = np.repeat(pk.centres, np.diff(pk.offsets), axis=0)
+    r2 = ((ctr[:, None, :] - ctr[None, :, :]) ** 2).sum(-1)
+    D = rng.standard_normal((n, n)) * np.exp(-0.3 * r2)
+    D = D + D.T
+    Q = oracle.schwarz(bs)
+    qs, keep, tau = _screen_keep(pk, Q, D)
+    assert 0.2 < keep.mean() < 0.8
+    Jr, Kr = oracle.jk_quartets(bs, D, qs[keep])
+    eng = DirectERI(bs, mol, device=0, schwarz_tau=0.0)
+    for _ in range(2):  # the second build reuses the work list and its item bounds
+        J, K = eng.jk(torch.tensor(D, device=DEV), dens_tau=tau)
+        np.testing.assert_allclose(J.cpu().numpy(), Jr, atol=1e-10)
+        np.testing.assert_allclose(K.cpu().numpy(), Kr, atol=1e-10)
+    # a density below every bound: nothing survives the compaction
+    J0, K0 = eng.jk(torch.tensor(D * 1e-30, device=DEV), dens_tau=tau)
+    assert float(J0.abs().max()) == 0.0 and float(K0.abs().max()) == 0.0
+
+
 def test_eri_tensor_spherical_vs_golden(golden):
     """6-31G** water in the solid-harmonic basis (the reference default):
     the tensor through the engine's spherical map against the reference's
