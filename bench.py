@@ -486,14 +486,25 @@ def kernel_configs(local: int):
             "values_per_s": n * 9 / sec, "ms": round(sec * 1e3, 3), "gbs": nbytes / sec / 1e9,
             "hbm_frac": nbytes / sec / 1e9 / hbm}
     del T
+    from jax_examples_b200 import flops
+    from jax_examples_b200.engine import fp_peak
+
     classes = {"(ss|ss)": (0, 0, 0, 0), "(pp|pp)": (1, 1, 1, 1), "(dd|dd)": (2, 2, 2, 2), "(ds|ps)": (2, 0, 1, 0)}
     nq = 1 << 20
     prim = {}
+    peak64 = fp_peak(False)
     for name, cls in classes.items():
         ex = torch.tensor(10 ** rng.uniform(-1, 2, (nq, 4)), device=dev)
         ctr = torch.tensor(rng.uniform(0, 4.0 / 0.529177210903, (nq, 4, 3)), device=dev)
         sec = timed(lambda: eri_prim_quartets(cls, ex, ctr), reps=2)
-        prim[name] = {"prim_quartets_per_s": nq / sec, "ms": round(sec * 1e3, 3)}
+        ne = 1
+        for l in cls:
+            ne *= (l + 1) * (l + 2) // 2
+        nbytes = nq * (16 + ne) * 8  # 4 exponents + 12 centre coordinates in, the block out
+        tf = nq * flops.prim_quartet_flops(*cls) / sec / 1e12
+        prim[name] = {"prim_quartets_per_s": nq / sec, "ms": round(sec * 1e3, 3), "gbs": round(nbytes / sec / 1e9, 1),
+                      "hbm_frac": round(nbytes / sec / 1e9 / hbm, 3), "model_tflops": round(tf, 2),
+                      "fp64_frac": round(tf / peak64, 3)}
         del ex, ctr
         torch.cuda.empty_cache()
     out["prim_quartets"] = prim

@@ -68,10 +68,21 @@ cudaError_t launch_schwarz(int pc, const SchwarzParams& p, cudaStream_t s) {
 // --------------------------------------------------------- primitive blocks
 // obara_saika.py:227-332 primitive_eri_block for a batch of primitive
 // quartets with unit coefficients (K_AB and K_CD included).
+//
+// A block of 128 threads takes kPrimQB = 128 / NS consecutive quartets, one
+// thread per (quartet, ket part).  The threads put their part of each block
+// into shared memory, and the block's kPrimQB x NAB x NCD outputs, one
+// contiguous run of the output array, are stored with consecutive threads on
+// consecutive addresses: a thread storing its own block element by element
+// would touch one cache line per lane in every store instruction.
+template <int NS>
+constexpr int prim_qb() { return NS >= 128 ? 1 : 128 / NS; }
+
 template <int LA, int LB, int LC, int LD, int NS>
 struct PrimBody {
   const PrimQuartetParams& prm;
   long long q;
+  double* blk;  // this quartet's NAB x NCD block in shared memory
 
   template <int PART>
   __device__ __forceinline__ void run() {
@@ -102,11 +113,10 @@ struct PrimBody {
     double ebuf[3][LA + 1][LB + 1][LA + LB + 1];
     quartet_accumulate<double, LA, LB, LC, LD, NS, PART, false, false>(&bra, 1, A, B, &ket, 1, C, D, prm.boys_al,
                                                                         ebuf, out);
-    double* o = prm.out + q * (Cfg::NAB * Cfg::NCD);
     static_for<Cfg::NAB * Cfg::NCDP>([&](auto x_) {
       constexpr int x = decltype(x_)::value;
       constexpr int ab = x / Cfg::NCDP, cdi = x % Cfg::NCDP;
-      o[ab * Cfg::NCD + Cfg::CD0 + cdi] = out[ab][cdi];
+      blk[ab * Cfg::NCD + Cfg::CD0 + cdi] = out[ab][cdi];
     });
   }
 };
@@ -114,10 +124,19 @@ struct PrimBody {
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) prim_kernel(const PrimQuartetParams prm) {
   constexpr int NS = class_split(LA, LB, LC, LD);
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= prm.n) return;
-  PrimBody<LA, LB, LC, LD, NS> body{prm, q};
-  dispatch_part<NS>(blockIdx.y, body);
+  constexpr int QB = prim_qb<NS>();
+  constexpr int NE = ncart(LA) * ncart(LB) * ncart(LC) * ncart(LD);
+  __shared__ double s_out[QB * NE];
+  const long long q0 = (long long)blockIdx.x * QB;
+  const int nq = (int)(prm.n - q0 < QB ? prm.n - q0 : QB);
+  const int ql = int(threadIdx.x) % QB, part = int(threadIdx.x) / QB;
+  if (ql < nq && part < NS) {
+    PrimBody<LA, LB, LC, LD, NS> body{prm, q0 + ql, s_out + ql * NE};
+    dispatch_part<NS>(part, body);
+  }
+  __syncthreads();
+  double* o = prm.out + q0 * NE;
+  for (int i = int(threadIdx.x); i < nq * NE; i += int(blockDim.x)) o[i] = s_out[i];
 }
 
 cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuartetParams& p, cudaStream_t s) {
@@ -125,13 +144,12 @@ cudaError_t launch_prim_quartets(int la, int lb, int lc, int ld, const PrimQuart
   if (la < lb || lc < ld || la > 2 || lc > 2) return cudaErrorInvalidValue;
   const int pb = pair_class(la, lb), pk = pair_class(lc, ld);
   if (pb < pk) return cudaErrorInvalidValue;
-  const unsigned gx = (unsigned)((p.n + 127) / 128);
   if (!is_reg_class(quartet_class(pb, pk))) return launch_col_prim(quartet_class(pb, pk), p, s);
   switch (quartet_class(pb, pk)) {
 #define X(Q, A, B, C, D)                                                                     \
   case Q: {                                                                                  \
-    dim3 grid(gx, class_split(A, B, C, D));                                                  \
-    prim_kernel<A, B, C, D><<<grid, 128, 0, s>>>(p);                                         \
+    constexpr long long qb = prim_qb<class_split(A, B, C, D)>();                            \
+    prim_kernel<A, B, C, D><<<(unsigned)((p.n + qb - 1) / qb), 128, 0, s>>>(p);              \
     return cudaGetLastError();                                                               \
   }
     JQC_FOR_REG_CLASSES(X)
