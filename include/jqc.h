@@ -14,6 +14,10 @@
  *   - Layout: basis functions in shell order, Cartesian components of a shell
  *     in libint order (lx descending, then ly descending), as
  *     jax_qc/integrals/mcmurchie_davidson.py:39-50 and overlap.py:58-64.
+ *   - A context's device scratch (density block maxima, the compacted work
+ *     items of screened builds, gradient force slots) is shared by all calls
+ *     on it: calls on one context must be ordered on the GPU (one stream, or
+ *     streams ordered by events).  Different contexts are independent.
  */
 #ifndef JQC_H_
 #define JQC_H_
