@@ -156,7 +156,7 @@ class Clocks:
 
 def batched_sweep(local: int, n_mol: int, seed: int = 2024):
     """Uneven-size geometry sweep: n_mol water clusters (1..12 waters,
-    +-0.1 A Gaussian noise) through one batched, autotuned, graph-replayed
+    +-0.1 A Gaussian noise) through one batched, graph-replayed
     mixed-precision RHF (incremental builds, FP64 tail) + screened gradient,
     against the same molecules one at a time on the plain FP64 path (a full
     FP64 build every iteration, unscreened gradient: the reference's
@@ -193,7 +193,10 @@ def batched_sweep(local: int, n_mol: int, seed: int = 2024):
     beng = BatchedERI(batch, schwarz_tau=SCHWARZ_TAU)
     torch.cuda.synchronize()
     t_ctx = time.perf_counter() - t_ctx
-    scf = run_rhf_batch(batch, chosen, engine=beng, use_graph=True, autotune=True)
+    # untuned launch shapes: on this sweep the autotuner saves 2% of the Fock
+    # seconds (0.605 against 0.617 s) for 1.6-5.2 s of tuning, which pays
+    # back only over many sweeps through its cache file
+    scf = run_rhf_batch(batch, chosen, engine=beng, use_graph=True, autotune=False)
     # the first gradient call also builds the gradient work list on the host;
     # the second is the kernel time (both sides are timed that way)
     first = {}
@@ -330,7 +333,7 @@ def _sequential_bfgs(local, mols, max_steps):
 def batched_bfgs(local: int, n_mol: int, steps: int = 10, seed: int = 2024, seq_every: int = 4):
     """The sweep's molecules (n_mol water clusters, 1..12 waters, +-0.1 A
     noise) optimised for ``steps`` BFGS steps each on the batched path: one
-    engine for the whole optimisation, autotuned once, geometry-only updates
+    engine for the whole optimisation, geometry-only updates
     between rounds, mixed precision with incremental builds, screened
     gradient.  Per-molecule energy and gradient error against FP64 at the
     final geometries (one batched plain-FP64 evaluation there).  Every
@@ -354,7 +357,7 @@ def batched_bfgs(local: int, n_mol: int, steps: int = 10, seed: int = 2024, seq_
         tm = {}
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = optimize_bfgs_batch(ms, BASIS, max_steps=steps, config=chosen, autotune=True, timing=tm)
+        res = optimize_bfgs_batch(ms, BASIS, max_steps=steps, config=chosen, autotune=False, timing=tm)
         torch.cuda.synchronize()
         return res, tm, time.perf_counter() - t0
 
@@ -401,7 +404,7 @@ def sharded_sweep(local: int, rank: int, world: int, n_mol: int, seed: int = 202
     """The uneven-size sweep (n_mol water clusters, 1..12 waters, +-0.1 A
     noise) sharded over the ranks: each rank takes a contiguous,
     cost-balanced share (``dist.sweep_shard``) and runs it as its own batch on
-    the chosen path (batched, autotuned, graph-replayed, mixed + incremental,
+    the chosen path (batched, graph-replayed, mixed + incremental,
     screened gradient).  No data-path collective; the times are the maximum
     over the ranks, from a barrier to the last rank's synchronize."""
     import torch
@@ -428,7 +431,7 @@ def sharded_sweep(local: int, rank: int, world: int, n_mol: int, seed: int = 202
     if mols:
         batch = MoleculeBatch(mols, BASIS)
         scf = run_rhf_batch(batch, chosen, engine=BatchedERI(batch, schwarz_tau=SCHWARZ_TAU), use_graph=True,
-                            autotune=True)
+                            autotune=False)
         tm = {}
         rhf_gradient_batch(batch, scf, tm, MIXED_GRAD_TAU)
         fock, grad = scf.record["jk_seconds"], tm["grad_seconds"]
