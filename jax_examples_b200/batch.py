@@ -311,6 +311,8 @@ class _BatchFock:
         self.D, self.J, self.K = eng.buffers(1)
         self.Jacc = torch.zeros_like(self.J[0])
         self.Kacc = torch.zeros_like(self.K[0])
+        self._flat_idx = {}  # molecule set -> flat indices of its blocks in D
+
         # molecules of the next build, read on the device by every build and
         # graph replay: the others are compacted out of the work lists
         self.n_mol = eng.engine.n_mol
@@ -319,6 +321,28 @@ class _BatchFock:
             self.active = torch.ones(self.n_mol, dtype=torch.int32, device=eng.device)
             self._active_host = np.ones(self.n_mol, dtype=np.int32)
             eng.engine.set_molecule_activity(self.active)
+
+    def _scatter(self, dens: dict, prev: Optional[dict] = None) -> None:
+        """D <- the blocks of ``dens`` (minus those of ``prev``), zero
+        elsewhere: one gather of the values and one indexed copy, not one
+        copy launch per molecule."""
+        ms = tuple(dens)
+        idx = self._flat_idx.get(ms)
+        if idx is None:
+            b, n = self.batch, self.D.shape[-1]
+            parts = []
+            for m in ms:
+                r = torch.arange(b.bf_off[m], b.bf_off[m] + b.n_bf[m], device=self.D.device, dtype=torch.int64)
+                parts.append((r[:, None] * n + r[None, :]).reshape(-1))
+            idx = torch.cat(parts) if parts else torch.zeros(0, dtype=torch.int64, device=self.D.device)
+            self._flat_idx[ms] = idx
+        self.D.zero_()
+        if not ms:
+            return
+        vals = torch.cat([dens[m].reshape(-1) for m in ms])
+        if prev is not None:
+            vals = vals - torch.cat([prev[m].reshape(-1) for m in ms])
+        self.D[0].view(-1).index_copy_(0, idx, vals)
 
     def _set_active(self, molecules) -> None:
         if self.active is None:
@@ -363,8 +387,7 @@ class _BatchFock:
         if not self.cart:
             return
         self._set_active(dens.keys())
-        for m, d in dens.items():
-            self.batch.block(self.D[0], m).copy_(d)
+        self._scatter(dens)
         prec, tau = self._settings(False)
         self.prep_times = {}
         if autotune:
@@ -405,18 +428,15 @@ class _BatchFock:
         periodic = not self.switched and self.since_full >= self.rebuild_every
         inc = self.incremental and self.prev is not None and not periodic and set(dens) <= set(self.prev)
         self._set_active(dens.keys())
-        self.D.zero_()
         if inc:
-            for m, d in dens.items():
-                b.block(self.D[0], m).copy_(d - self.prev[m])
+            self._scatter(dens, self.prev)
             self._launch(True)
             self.Jacc += self.J[0]
             self.Kacc += self.K[0]
             self.since_full += 1
             self.log["incremental_builds"] += 1
         else:
-            for m, d in dens.items():
-                b.block(self.D[0], m).copy_(d)
+            self._scatter(dens)
             self._launch(False)
             self.Jacc.copy_(self.J[0])
             self.Kacc.copy_(self.K[0])
@@ -635,9 +655,24 @@ def run_rhf_batch(batch: MoleculeBatch, config: Optional[CalcConfig] = None, eng
         groups.append(_Group(members, S, H, no))
     fb = _BatchFock(eng, batch, config, use_graph)
 
+    if fb.cart:
+        # flat indices of every group's blocks in the batch matrices: J and K
+        # of a whole group are one gather each from the builder's accumulators
+        N = batch.n_basis
+        for g in groups:
+            r = torch.stack([torch.arange(batch.bf_off[m], batch.bf_off[m] + batch.n_bf[m], device=g.H.device)
+                             for m in g.members])
+            g.flat = r[:, :, None] * N + r[:, None, :]
+
     def fock(g: _Group, jk: dict, fallback):
-        J = torch.stack([jk[m][0] if m in jk else fallback[i] * 0 for i, m in enumerate(g.members)])
-        K = torch.stack([jk[m][1] if m in jk else fallback[i] * 0 for i, m in enumerate(g.members)])
+        if fb.cart:
+            # members that left the builds keep their last J/K there; their
+            # state is not updated any more (masked below)
+            J = fb.Jacc.view(-1)[g.flat]
+            K = fb.Kacc.view(-1)[g.flat]
+        else:
+            J = torch.stack([jk[m][0] if m in jk else fallback[i] * 0 for i, m in enumerate(g.members)])
+            K = torch.stack([jk[m][1] if m in jk else fallback[i] * 0 for i, m in enumerate(g.members)])
         return g.H + J - 0.5 * K
 
     # core guess (rhf.py:111-121)

@@ -152,3 +152,29 @@ def test_pooled_eigensolver_matches_per_matrix_eigh():
                 torch.testing.assert_close(C[i].T @ (Xi @ Xi) @ C[i], torch.eye(F.shape[-1], dtype=F.dtype),
                                            rtol=0, atol=1e-10)
     assert torch.get_num_threads() == n_threads  # the caller's solver threads are left as they were
+
+
+def test_batch_density_scatter_matches_block_copies():
+    """_BatchFock writes the active molecules' densities (or density changes)
+    into the batch buffer with one indexed copy: the same matrix as one
+    block copy per molecule, zero outside the active blocks."""
+    import torch
+
+    mols = [pb.water_cluster(n, seed=5 + n) for n in (1, 2, 1)]
+    batch = jb.MoleculeBatch(mols, "sto-3g")
+    N = batch.n_basis
+    fb = jb._BatchFock.__new__(jb._BatchFock)
+    fb.batch = batch
+    fb.D = torch.full((1, N, N), 7.0, dtype=torch.float64)
+    fb._flat_idx = {}
+    g = torch.Generator().manual_seed(3)
+    dens = {m: torch.rand((batch.n_bf[m],) * 2, generator=g, dtype=torch.float64) for m in (2, 0)}
+    prev = {m: torch.rand((batch.n_bf[m],) * 2, generator=g, dtype=torch.float64) for m in (2, 0)}
+    for p in (None, prev):
+        fb._scatter(dens, p)
+        ref = torch.zeros((N, N), dtype=torch.float64)
+        for m, d in dens.items():
+            batch.block(ref, m).copy_(d if p is None else d - p[m])
+        assert torch.equal(fb.D[0], ref)
+    fb._scatter({})
+    assert float(fb.D.abs().max()) == 0.0
